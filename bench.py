@@ -1,0 +1,474 @@
+"""Benchmark: in-place 3D R2C then C2R of a 512^3 FP32 field on one B200.
+
+Workload (the reference's headline case, GPU_FFT's INIT_GPU_FFT +
+GPU_FFT_R2C + GPU_FFT_C2R at procs=1): a seeded i.i.d. N(0,1) real field of
+512x512x512 in the padded layout [512][512][514] float32, resident in HBM;
+one step = one forward R2C plus one inverse C2R, in place (the inverse leaves
+N^3 * f, so the same buffer is transformed every step).  The field is 539 MB,
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+The JSON line reports, per the project's bench contract:
+  value / ms_per_step   device time per R2C+C2R (CUDA events on the launching
+                        stream, mean over K timed steps, max over ranks);
+  e2e                   the same step through the C ABI with host buffers:
+                        pinned H2D copy of the field, R2C, C2R, D2H copy;
+  roofline              the dominant kernel's algorithmic bytes per launch
+                        (2*S: one read and one write of the field) over its
+                        mean launch time, against the measured HBM copy peak;
+  cpu_baseline          the FP64 C oracle (oracle/fft_oracle.c, all host
+                        threads) on a bounded sample, scaled to one step.
+--impl reference times the reference's own implementation of this path:
+GPU_FFT built from its sources at procs=1 (oracle/_ref, cuFFT on the GPU,
+through GPU_FFT::INIT_GPU_FFT / GPU_FFT_R2C / GPU_FFT_C2R); it has no CPU
+implementation.  Without oracle/_ref it times the C oracle on the host cores.
+With N > 1 (torchrun) every rank runs its own independent replica: the
+transform does not shard on one GPU per process here.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = NZ = 512
+DTYPE = "float"
+
+
+def field_bytes(nx, ny, nz, dt):
+    return nx * ny * (nz // 2 + 1) * (8 if dt == "float" else 16)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+def dist_setup(gpus: int):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_field(nx, ny, nz, dt, seed=20240611):
+    import torch
+
+    tdt = torch.float32 if dt == "float" else torch.float64
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    f = torch.zeros((nx, ny, 2 * (nz // 2 + 1)), dtype=tdt, device="cuda")
+    f[:, :, :nz] = torch.randn((nx, ny, nz), generator=gen, dtype=tdt, device="cuda")
+    return f
+
+
+# ---------------------------------------------------------------------------
+# timing helpers
+# ---------------------------------------------------------------------------
+def time_steps(step_fn, steps, warmup, world, stream):
+    """W untimed steps, then K steps bracketed by barrier + synchronize; per-step
+    CUDA events on `stream`.  Returns (total_ms, per-step ms list)."""
+    import torch
+
+    for _ in range(warmup):
+        step_fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for i in range(steps):
+        step_fn()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    return evs[0].elapsed_time(evs[-1]), per
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 C oracle on the host cores, bounded sample
+# ---------------------------------------------------------------------------
+def cpu_baseline(nx, ny, nz, budget_s=25.0):
+    from oracle import oracle as o
+
+    o.build_c_oracle()
+    threads = o.c_max_threads()
+    # calibrate on a 128^3 R2C+C2R, then run the largest cubic grid (<= the
+    # workload) whose extrapolated time fits the budget and scale by
+    # N log N to the workload
+    def run(n):
+        f = o.normal_field(n, n, n, seed=1, dtype=np.float64)
+        t0 = time.perf_counter()
+        s = o.c_r2c(f, n, n, n, threads=threads, steps=False)
+        o.c_c2r(s, n, n, n, threads=threads, steps=False)
+        return time.perf_counter() - t0
+
+    def work(n0, n1, n2):
+        return n0 * n1 * n2 * np.log2(float(n0) * n1 * n2)
+
+    n = 128
+    t = run(n)
+    while n < max(nx, ny, nz) and t * work(2 * n, 2 * n, 2 * n) / work(n, n, n) < budget_s:
+        n *= 2
+        t = run(n)
+    scale = work(nx, ny, nz) / work(n, n, n)
+    return {"value": t * scale * 1e3, "unit": "ms", "cores": threads, "kind": "port",
+            "sample": f"FP64 C oracle R2C+C2R of a {n}^3 N(0,1) field on {threads} threads "
+                      f"({t:.2f} s), scaled by N log N to {nx}x{ny}x{nz}"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank):
+    import torch
+    import gpu_fft_b200 as g
+
+    nx, ny, nz, dt = args.nx, args.ny, args.nz, args.dtype
+    S = field_bytes(nx, ny, nz, dt)
+    plan = g.Plan(nx, ny, nz, dt)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    f = make_field(nx, ny, nz, dt)
+    ptr = f.data_ptr()
+    scale = 1.0 / (nx * ny * nz)
+
+    def step():
+        plan.r2c_ptr(ptr, sh)
+        plan.c2r_ptr(ptr, sh)
+
+    # keep values bounded across many steps: C2R multiplies by N^3
+    def renorm():
+        f.mul_(scale)
+
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    for _ in range(args.warmup):  # untimed warm-up
+        renorm()
+        step()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    # Timed region: K steps of R2C + C2R.  Each step multiplies the field by
+    # N^3, so float32 stays finite for at most 4 consecutive steps: the K steps
+    # run in chunks of <= 4, each bracketed by barrier + synchronize, with the
+    # field rescaled between chunks outside the timed spans.
+    total_ms, per, done = 0.0, [], 0
+    while done < args.steps:
+        k = min(4, args.steps - done)
+        renorm()
+        t, p = time_steps(step, k, 0, world, stream)
+        total_ms += t
+        per += p
+        done += k
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(world, total_ms / args.steps)
+
+    # per-kernel breakdown (same stream, CUDA events between launches)
+    kt = {("A", True): [], ("B", True): [], ("B", False): [], ("A", False): []}
+    renorm()
+    torch.cuda.synchronize()
+    for it in range(max(5, min(args.steps, 20))):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        evs[0].record(stream)
+        plan.pass_ptr(ptr, sh, 0, True)
+        evs[1].record(stream)
+        plan.pass_ptr(ptr, sh, 1, True)
+        evs[2].record(stream)
+        plan.pass_ptr(ptr, sh, 1, False)
+        evs[3].record(stream)
+        plan.pass_ptr(ptr, sh, 0, False)
+        evs[4].record(stream)
+        torch.cuda.synchronize()
+        if it >= 2:
+            for i, key in enumerate(kt):
+                kt[key].append(evs[i].elapsed_time(evs[i + 1]))
+        f.mul_(scale)
+    kmean = {f"pass_{k[0]}_{'fwd' if k[1] else 'inv'}": statistics.mean(v) for k, v in kt.items()}
+    dom = max(kmean, key=kmean.get)
+    peak, peak_kind = load_peaks()
+    achieved = 2 * S / (kmean[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "kernel": dom,
+                "algorithmic_bytes_per_launch": 2 * S, "peak_source": peak_kind,
+                "kernel_ms": {k: round(v, 4) for k, v in kmean.items()}}
+    step_bytes = 8 * S  # 2 transforms x (2 passes x (read + write) of S)
+
+    # e2e through the C ABI with host buffers (pinned): H2D, R2C, C2R, D2H
+    host_in = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+    host_in.copy_(f.cpu())
+    host_out = torch.empty_like(host_in, pin_memory=True)
+
+    def e2e_step():
+        f.copy_(host_in, non_blocking=True)
+        plan.r2c_ptr(ptr, sh)
+        plan.c2r_ptr(ptr, sh)
+        host_out.copy_(f, non_blocking=True)
+
+    e2e_steps = max(3, min(args.steps, 10))
+    e_total, _ = time_steps(e2e_step, e2e_steps, 2, world, stream)
+    e2e_ms = max_over_ranks(world, e_total / e2e_steps)
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": f"R2C+C2R {nx}x{ny}x{nz} {'FP32' if dt == 'float' else 'FP64'} ms per step",
+            "value": round(ms, 4),
+            "unit": "ms",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if dt == "float" else "f64",
+            "data": "synthetic: seeded i.i.d. N(0,1) real field, padded layout, device-resident",
+            "config": {"workload": f"in-place R2C+C2R, {nx}x{ny}x{nz} {dt}, procs=1 per GPU",
+                       "grid": [nx, ny, nz], "field_bytes": S, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (539 MB field vs 126 MB L2); no flush"},
+            "p50_ms": round(pct(per, 50), 4),
+            "p99_ms": round(pct(per, 99), 4),
+            "hbm_gbs_8S": round(step_bytes / (ms * 1e-3) / 1e9, 1),
+            "roofline_8S_frac": round(step_bytes / (ms * 1e-3) / 1e9 / peak, 4),
+            "roofline": roofline,
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": S, "d2h_bytes_per_step": S},
+            "gpu_launches": 2 * plan.launches() * args.steps,
+            "clocks": clocks,
+            "plan": plan.describe(),
+        }
+    return result
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    import ctypes
+
+    import torch
+
+    nx, ny, nz, dt = args.nx, args.ny, args.nz, args.dtype
+    S = field_bytes(nx, ny, nz, dt)
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libref_api.so")
+    base = {"impl": "reference", "metric": f"R2C+C2R {nx}x{ny}x{nz} {'FP32' if dt == 'float' else 'FP64'} ms per step",
+            "unit": "ms", "higher_is_better": False, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if dt == "float" else "f64",
+            "data": "synthetic: seeded i.i.d. N(0,1) real field, padded layout",
+            "config": {"workload": f"in-place R2C+C2R, {nx}x{ny}x{nz} {dt}, procs=1 per GPU", "grid": [nx, ny, nz],
+                       "field_bytes": S, "parallelism": f"replicas x{world}"}}
+    if not os.path.exists(lib_path):
+        if rank != 0:
+            return None
+        cb = cpu_baseline(nx, ny, nz)
+        base.update({"value": round(cb["value"], 3), "ms_per_step": round(cb["value"], 3), "cpu_baseline": cb,
+                     "e2e": {"value": round(cb["value"], 3), "unit": "ms", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0},
+                     "note": "oracle/_ref not built: timed the FP64 C oracle port on the host cores"})
+        return base
+    lib = ctypes.CDLL(lib_path)
+    lib.ref_init.argtypes = [ctypes.c_longlong] * 3 + [ctypes.c_int]
+    lib.ref_r2c.argtypes = [ctypes.c_int, ctypes.c_void_p]
+    lib.ref_c2r.argtypes = [ctypes.c_int, ctypes.c_void_p]
+    is_d = 0 if dt == "float" else 1
+    rc = lib.ref_init(nx, ny, nz, is_d)
+    if rc != 0:
+        raise RuntimeError(f"reference INIT_GPU_FFT failed: cuda error {rc}")
+    stream = torch.cuda.current_stream()  # the legacy default stream, which the reference uses
+    f = make_field(nx, ny, nz, dt)
+    ptr = f.data_ptr()
+    scale = 1.0 / (nx * ny * nz)
+
+    def step():
+        lib.ref_r2c(is_d, ptr)
+        lib.ref_c2r(is_d, ptr)
+
+    for _ in range(args.warmup):
+        f.mul_(scale)
+        step()
+    torch.cuda.synchronize()
+    total_ms, per, done = 0.0, [], 0
+    while done < args.steps:
+        k = min(4, args.steps - done)
+        f.mul_(scale)
+        t, p = time_steps(step, k, 0, world, stream)
+        total_ms += t
+        per += p
+        done += k
+    ms = max_over_ranks(world, total_ms / args.steps)
+    host_in = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+    host_in.copy_(f.cpu())
+    host_out = torch.empty_like(host_in, pin_memory=True)
+
+    def e2e_step():
+        f.copy_(host_in, non_blocking=True)
+        lib.ref_r2c(is_d, ptr)
+        lib.ref_c2r(is_d, ptr)
+        host_out.copy_(f, non_blocking=True)
+
+    e_steps = max(3, min(args.steps, 10))
+    e_total, _ = time_steps(e2e_step, e_steps, 2, world, stream)
+    e2e_ms = max_over_ranks(world, e_total / e_steps)
+    if rank != 0:
+        return None
+    base.update({
+        "value": round(ms, 4), "ms_per_step": round(ms, 4), "p50_ms": round(pct(per, 50), 4),
+        "p99_ms": round(pct(per, 99), 4),
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": S, "d2h_bytes_per_step": S},
+        "cpu_baseline": {"value": round(ms, 4), "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "GPU_FFT built from its sources at procs=1 (cuFFT + its permutation kernels), "
+                                   "the full workload every step; the reference has no CPU implementation, so "
+                                   "its own code runs on the GPU (one host thread drives it)"},
+    })
+    return base
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--nz", type=int, default=NZ)
+    ap.add_argument("--dtype", choices=["float", "double"], default=DTYPE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, _ = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, world, rank)
+        else:
+            res = run_ours(args, world, rank)
+            if rank == 0 and res is not None:
+                if world == 1 and not args.no_cpu_baseline:
+                    res["cpu_baseline"] = cpu_baseline(args.nx, args.ny, args.nz)
+                else:
+                    res["cpu_baseline"] = None
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+"""gpu_fft_b200 — Python binding of libgpufft_b200.so (B200-native 3D R2C/C2R).
+
+A thin ctypes layer over the C ABI in include/gpufft_b200.h; torch supplies
+device memory and streams.  The names mirror GPU_FFT's C++ API
+(GPU_FFT/src/GPU_FFT/GPU_FFT.h:111-121):
+
+    INIT_GPU_FFT(Nx, Ny, Nz, procs=1, rank=0, dtype="float")
+    GPU_FFT_R2C(field)      # in place, float32/float64 padded real field
+    GPU_FFT_C2R(field)      # in place, the inverse (unnormalised)
+
+plus a ``Plan`` object for several grids/precisions at once.  There is no
+fallback: if the CUDA library is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgpufft_b200.so")
+
+GPUFFT_FLOAT = 0
+GPUFFT_DOUBLE = 1
+STATUS = {0: "SUCCESS", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NOT_INIT", 5: "ERR_OOM"}
+
+# every symbol include/gpufft_b200.h declares
+EXPORTS = (
+    "gpufft_init", "gpufft_r2c", "gpufft_c2r", "gpufft_finalize", "gpufft_last_error",
+    "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_exec_r2c", "gpufft_exec_c2r",
+    "gpufft_exec_pass", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
+)
+
+_lib = None
+
+
+class GpuFFTError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libgpufft_b200.so; raises if it was not built (no silent fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libgpufft_b200.so not found at {path}; build it with `python -m gpu_fft_b200.build`")
+    lib = ctypes.CDLL(path)
+    i64, vp, ci = ctypes.c_int64, ctypes.c_void_p, ctypes.c_int
+    lib.gpufft_init.argtypes = [i64, i64, i64, ci, ci, ci]
+    lib.gpufft_r2c.argtypes = [ci, vp, vp]
+    lib.gpufft_c2r.argtypes = [ci, vp, vp]
+    lib.gpufft_finalize.argtypes = []
+    lib.gpufft_last_error.restype = ctypes.c_char_p
+    lib.gpufft_plan_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci]
+    lib.gpufft_plan_destroy.argtypes = [vp]
+    lib.gpufft_exec_r2c.argtypes = [vp, vp, vp]
+    lib.gpufft_exec_c2r.argtypes = [vp, vp, vp]
+    lib.gpufft_exec_pass.argtypes = [vp, vp, vp, ci, ci]
+    lib.gpufft_field_bytes.argtypes = [i64, i64, i64, ci]
+    lib.gpufft_field_bytes.restype = i64
+    lib.gpufft_plan_launches.argtypes = [vp]
+    lib.gpufft_plan_describe.argtypes = [vp, ctypes.c_char_p, ci]
+    for name in EXPORTS:
+        if getattr(lib, name, None) is None:
+            raise ImportError(f"{path} does not export {name}")
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise GpuFFTError(rc, load_library().gpufft_last_error().decode())
+
+
+def _dtype_code(dtype) -> int:
+    s = str(dtype)
+    if s in ("float", "float32", "torch.float32", "f32", "0"):
+        return GPUFFT_FLOAT
+    if s in ("double", "float64", "torch.float64", "f64", "1"):
+        return GPUFFT_DOUBLE
+    raise ValueError(f"unsupported dtype {dtype!r}: float/float32 or double/float64")
+
+
+def _stream_handle(stream) -> int:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+
+
+def nh_of(nz: int) -> int:
+    return nz // 2 + 1
+
+
+def field_shape(nx: int, ny: int, nz: int) -> tuple:
+    """Shape of the padded real field: (Nx, Ny, 2*(Nz//2+1))."""
+    return (nx, ny, 2 * nh_of(nz))
+
+
+def field_bytes(nx: int, ny: int, nz: int, dtype="float") -> int:
+    return int(load_library().gpufft_field_bytes(nx, ny, nz, _dtype_code(dtype)))
+
+
+class Plan:
+    """A plan for one grid and precision (gpufft_plan_create)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, dtype="float"):
+        lib = load_library()
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.dtype_code = _dtype_code(dtype)
+        h = ctypes.c_void_p()
+        _check(lib.gpufft_plan_create(ctypes.byref(h), self.nx, self.ny, self.nz, self.dtype_code))
+        self._h = h
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value or 0)
+
+    def _ptr(self, field) -> int:
+        import torch
+
+        want = torch.float32 if self.dtype_code == GPUFFT_FLOAT else torch.float64
+        if field.dtype not in (want, torch.complex64 if want == torch.float32 else torch.complex128):
+            raise TypeError(f"field dtype {field.dtype} does not match the plan's {want}")
+        if not field.is_cuda or not field.is_contiguous():
+            raise ValueError("field must be a contiguous CUDA tensor")
+        need = self.nx * self.ny * nh_of(self.nz) * (8 if self.dtype_code == GPUFFT_FLOAT else 16)
+        if field.numel() * field.element_size() < need:
+            raise ValueError(f"field holds {field.numel() * field.element_size()} bytes, the grid needs {need}")
+        return field.data_ptr()
+
+    def r2c(self, field, stream=None):
+        _check(load_library().gpufft_exec_r2c(self._h, self._ptr(field), _stream_handle(stream)))
+        return field
+
+    def c2r(self, field, stream=None):
+        _check(load_library().gpufft_exec_c2r(self._h, self._ptr(field), _stream_handle(stream)))
+        return field
+
+    def r2c_ptr(self, ptr: int, stream: int = 0) -> None:
+        _check(load_library().gpufft_exec_r2c(self._h, ptr, stream))
+
+    def c2r_ptr(self, ptr: int, stream: int = 0) -> None:
+        _check(load_library().gpufft_exec_c2r(self._h, ptr, stream))
+
+    def pass_ptr(self, ptr: int, stream: int, which: int, forward: bool) -> None:
+        """Launch one kernel of the transform: which=0 Pass A (z,y), 1 Pass B (x)."""
+        _check(load_library().gpufft_exec_pass(self._h, ptr, stream, int(which), 1 if forward else 0))
+
+    def launches(self) -> int:
+        return int(load_library().gpufft_plan_launches(self._h))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        load_library().gpufft_plan_describe(self._h, buf, 1024)
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# reference-shaped API (GPU_FFT::INIT_GPU_FFT / GPU_FFT_R2C / GPU_FFT_C2R)
+# ---------------------------------------------------------------------------
+def INIT_GPU_FFT(nx: int, ny: int, nz: int, procs: int = 1, rank: int = 0, dtype="float") -> None:
+    """GPU_FFT::INIT_GPU_FFT<T1,T2>(Nx,Ny,Nz,procs,rank,comm) (GPU_FFT_init.cu:41-93)."""
+    _check(load_library().gpufft_init(int(nx), int(ny), int(nz), _dtype_code(dtype), int(procs), int(rank)))
+
+
+def _field_dtype(field) -> int:
+    import torch
+
+    if field.dtype in (torch.float32, torch.complex64):
+        return GPUFFT_FLOAT
+    if field.dtype in (torch.float64, torch.complex128):
+        return GPUFFT_DOUBLE
+    raise TypeError(f"unsupported field dtype {field.dtype}")
+
+
+def GPU_FFT_R2C(field, stream=None):
+    """GPU_FFT::GPU_FFT_R2C<T1,T2>(T1*) (FFT_R2C.cu:41-70), in place."""
+    if not field.is_cuda or not field.is_contiguous():
+        raise ValueError("field must be a contiguous CUDA tensor")
+    _check(load_library().gpufft_r2c(_field_dtype(field), field.data_ptr(), _stream_handle(stream)))
+    return field
+
+
+def GPU_FFT_C2R(field, stream=None):
+    """GPU_FFT::GPU_FFT_C2R<T1,T2>(T2*) (FFT_C2R.cu:41-70), in place."""
+    if not field.is_cuda or not field.is_contiguous():
+        raise ValueError("field must be a contiguous CUDA tensor")
+    _check(load_library().gpufft_c2r(_field_dtype(field), field.data_ptr(), _stream_handle(stream)))
+    return field
+
+
+def finalize() -> None:
+    _check(load_library().gpufft_finalize())

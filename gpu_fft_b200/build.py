@@ -1,0 +1,57 @@
+"""Build recipe for libgpufft_b200.so (nvcc, sm_100a, in-tree).
+
+``python -m gpu_fft_b200.build`` compiles every CUDA source of the library
+into ``gpu_fft_b200/libgpufft_b200.so``.  nvcc cross-compiles for sm_100a
+without a GPU present, so this runs on build hosts too.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libgpufft_b200.so")
+
+SOURCES = ["gpufft.cu"]
+HEADERS = ["fft_kernels.cuh", "fft_radix.cuh", "gpufft_internal.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else "nvcc"
+
+
+def _inputs() -> list[str]:
+    files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    files.append(os.path.join(ROOT, "include", "gpufft_b200.h"))
+    return files
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(f) <= t for f in _inputs())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    srcs = [os.path.join(CSRC, f) for f in SOURCES]
+    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,478 @@
+// gpufft.cu — host side of libgpufft_b200.so: plans, twiddle tables, launches
+// and the C ABI declared in include/gpufft_b200.h.
+//
+// A plan replaces what GPU_FFT's INIT_GPU_FFT sets up
+// (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT_init.cu:41-93): instead of three
+// cuFFT plans and a field-sized scratch buffer it holds a radix factorisation
+// per axis, the tile shapes of the two passes, the cluster size of Pass A and
+// three FP64-computed twiddle tables (rounded once to the storage type).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gpufft_b200.h"
+#include "fft_kernels.cuh"
+#include "gpufft_internal.h"
+
+namespace gpufft {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+const char *last_error() { return g_last_error.c_str(); }
+
+static int cuda_error(cudaError_t e, const char *what) {
+    return set_error(GPUFFT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// factorisation and tile feasibility
+// ---------------------------------------------------------------------------
+// Radix list for a length-n FFT: the power-of-two part split into as few
+// stages of at most 16 as possible with balanced sizes (512 -> 8,8,8;
+// 1024 -> 16,8,8), then the odd prime factors 3, 5, 7, 11, 13.
+bool factorize(int n, std::vector<int> &radices) {
+    radices.clear();
+    if (n < 1) return false;
+    int a = 0, r = n;
+    while (r % 2 == 0) { r /= 2; ++a; }
+    if (a > 0) {
+        const int k = (a + 3) / 4;
+        for (int s = 0; s < k; ++s) {
+            const int bits = a / k + (s < a % k ? 1 : 0);
+            radices.push_back(1 << bits);
+        }
+    }
+    for (int p : {3, 5, 7, 11, 13})
+        while (r % p == 0) { radices.push_back(p); r /= p; }
+    return r == 1;
+}
+
+static void fill_axis(AxisPlan &ax, int n, const std::vector<int> &radices, int tabmul) {
+    std::memset(&ax, 0, sizeof(ax));
+    ax.n = n;
+    ax.nst = (int)radices.size();
+    int p = 1;
+    for (int s = 0; s < ax.nst; ++s) {
+        const int R = radices[s];
+        ax.radix[s] = R;
+        ax.p[s] = p;
+        ax.pdiv[s] = make_fastdiv((uint32_t)p);
+        ax.twstep[s] = tabmul * (n / (p * R));
+        p *= R;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// twiddle tables: w[e] = exp(-2 pi i e / L), e < L, computed in long double
+// on the reduced angle and rounded once to the storage type
+// ---------------------------------------------------------------------------
+template <typename T>
+static std::vector<T> twiddle_table(int L) {
+    std::vector<T> t(2 * (size_t)L);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int e = 0; e < L; ++e) {
+        const long double ang = two_pi * (long double)e / (long double)L;
+        t[2 * e] = (T)cosl(ang);
+        t[2 * e + 1] = (T)(-sinl(ang));
+    }
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+static int device_sms(int dev) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 1;
+}
+
+template <typename T>
+static int build_plan(Plan &P) {
+    using V = cx_t<T>;
+    const int vs = (int)sizeof(V);
+    const int maxe = MaxE<T>::value;
+    const int nx = (int)P.nx, ny = (int)P.ny, nz = (int)P.nz, m = nz / 2, nh = nz / 2 + 1;
+    std::vector<int> rx, ry, rz;
+    if (!factorize(nx, rx) || !factorize(ny, ry) || !factorize(m, rz))
+        return set_error(GPUFFT_ERR_UNSUPPORTED,
+                         "grid %dx%dx%d: Nx, Ny and Nz/2 must factor into 2,3,5,7,11,13", nx, ny, nz);
+
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.device);
+    if (smem_optin <= 0) smem_optin = 227 * 1024;
+    const int budget = smem_optin - 1024;
+
+    // Tiles are sized so that both ping-pong tiles plus the twiddle tables
+    // take about a third of the SM's shared memory (three CTAs per SM), with
+    // rows of at most 128 bytes; long axes shrink the tile width down to 1.
+    const long long target = std::min<long long>(budget, 75 * 1024);
+    const int wmax = 128 / vs;
+
+    // ---- Pass B (x axis): column tiles of wx columns, [nx][wx] in smem
+    int wx = wmax;
+    while (wx > 1 && (long long)(nx + 2LL * nx * wx) * vs > target) wx /= 2;
+    if ((long long)(nx + 2LL * nx * wx) * vs > budget)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "Nx=%d too long for one shared-memory tile", nx);
+
+    // ---- Pass A phase 2 (y axis)
+    int wy = wmax;
+    while (wy > 1 && (long long)(nz + ny + 2LL * ny * wy) * vs > target) wy /= 2;
+    if ((long long)(nz + ny + 2LL * ny * wy) * vs > budget)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "Ny=%d too long for one shared-memory tile", ny);
+
+    // ---- Pass A phase 1 (z rows): odd pitch >= m+1 keeps row accesses conflict-free
+    const int pz = (m % 2 == 0) ? m + 1 : m + 2;
+    int wz = 32;
+    auto bytes_a = [&](int wzc) {
+        return (long long)(nz + ny + 2LL * std::max<long long>((long long)wzc * pz, (long long)ny * wy)) * vs;
+    };
+    while (wz > 1 && bytes_a(wz) > target) wz = (wz > 16) ? wz - 8 : wz / 2;
+    if (bytes_a(wz) > budget) return set_error(GPUFFT_ERR_UNSUPPORTED, "Nz=%d too long for one shared-memory tile", nz);
+    (void)maxe;
+
+    // ---- parameters
+    PassAParams &A = P.pa;
+    std::memset(&A, 0, sizeof(A));
+    A.nx = nx; A.ny = ny; A.nz = nz; A.nh = nh; A.m = m;
+    A.wz = wz; A.pz = pz; A.wzdiv = make_fastdiv(wz); A.nhdiv = make_fastdiv(nh);
+    A.wy = wy; A.wydiv = make_fastdiv(wy);
+    fill_axis(A.az, m, rz, 2);
+    fill_axis(A.ay, ny, ry, 1);
+    A.tile_elems = std::max(wz * pz, ny * wy);
+    P.smem_a = (size_t)(nz + ny + 2 * (size_t)A.tile_elems) * vs;
+
+    PassBParams &B = P.pb;
+    std::memset(&B, 0, sizeof(B));
+    B.nx = nx; B.ncols = (long long)ny * nh; B.wx = wx; B.wxdiv = make_fastdiv(wx);
+    fill_axis(B.ax, nx, rx, 1);
+    B.ntiles = (B.ncols + wx - 1) / wx;
+    P.smem_b = (size_t)(nx + 2 * (size_t)nx * wx) * vs;
+
+    // ---- twiddle tables on the device
+    const std::vector<T> hx = twiddle_table<T>(nx), hy = twiddle_table<T>(ny), hz = twiddle_table<T>(nz);
+    const size_t bx = hx.size() * sizeof(T), by = hy.size() * sizeof(T), bz = hz.size() * sizeof(T);
+    cudaError_t e = cudaMalloc(&P.tw_dev, bx + by + bz);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_OOM, "cudaMalloc twiddles: %s", cudaGetErrorString(e));
+    char *base = (char *)P.tw_dev;
+    e = cudaMemcpy(base, hx.data(), bx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + bx, hy.data(), by, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + bx + by, hz.data(), bz, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpy twiddles");
+    B.twx = base;
+    A.twy = base + bx;
+    A.twz = base + bx + by;
+
+    // ---- kernel attributes and launch geometry
+    auto ka_f = pass_a_kernel<T, true>, ka_i = pass_a_kernel<T, false>;
+    auto kb_f = pass_b_kernel<T, true>, kb_i = pass_b_kernel<T, false>;
+    for (auto k : {ka_f, ka_i}) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_a);
+        if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(pass A smem)");
+        cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
+    for (auto k : {kb_f, kb_i}) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_b);
+        if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(pass B smem)");
+    }
+    const int sms = device_sms(P.device);
+    int occ_a = 0, occ_b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, ka_f, kThreads, P.smem_a);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, kb_f, kThreads, P.smem_b);
+    occ_a = std::max(occ_a, 1);
+    occ_b = std::max(occ_b, 1);
+
+    // Cluster size: enough CTAs per plane that the planes in flight fit in
+    // about half of L2, and enough clusters in total to fill the GPU; at most
+    // 8 (the portable cluster limit) and at most one column tile per CTA.
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, P.device);
+    if (l2 <= 0) l2 = 96 << 20;
+    const long long plane_bytes = (long long)ny * nh * vs;
+    const int resident = occ_a * sms;
+    const int tiles_y = (m + wy - 1) / wy;
+    const int kcap = std::max(1, std::min({8, tiles_y, ny}));
+    int K = 1;
+    while (K < kcap && (long long)(resident / K) * plane_bytes > (long long)l2 / 2) K *= 2;
+    while (K < kcap && (long long)nx * K < resident) K *= 2;
+    K = std::min(K, kcap);
+    A.K = K;
+
+    int max_clusters = 0;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim = dim3(K * std::max(1, nx), 1, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = P.smem_a;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = K;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaOccupancyMaxActiveClusters(&max_clusters, ka_f, &cfg);
+        if (e != cudaSuccess || max_clusters < 1) max_clusters = std::max(1, resident / K);
+    }
+    P.grid_a = K * std::min(nx, max_clusters);
+    P.grid_b = (int)std::min<long long>(B.ntiles, (long long)occ_b * sms);
+    P.occ_a = occ_a;
+    P.occ_b = occ_b;
+    return GPUFFT_SUCCESS;
+}
+
+int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype) {
+    if (!out) return set_error(GPUFFT_ERR_INVALID, "plan pointer is NULL");
+    *out = nullptr;
+    if (nx < 1 || ny < 1 || nz < 1)
+        return set_error(GPUFFT_ERR_INVALID, "grid %lldx%lldx%lld: every size must be >= 1", (long long)nx,
+                         (long long)ny, (long long)nz);
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE)
+        return set_error(GPUFFT_ERR_INVALID, "dtype %d is neither GPUFFT_FLOAT nor GPUFFT_DOUBLE", dtype);
+    if (nz % 2 != 0)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "odd Nz=%lld is not supported", (long long)nz);
+    if (nx > (1 << 24) || ny > (1 << 24) || nz > (1 << 24) || ny * (nz / 2 + 1) >= (1LL << 31))
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "grid too large for 32-bit in-plane indexing");
+    Plan *P = new (std::nothrow) Plan();
+    if (!P) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
+    P->nx = nx; P->ny = ny; P->nz = nz; P->dtype = dtype;
+    cudaError_t e = cudaGetDevice(&P->device);
+    if (e != cudaSuccess) { delete P; return cuda_error(e, "cudaGetDevice"); }
+    const int rc = dtype == GPUFFT_FLOAT ? build_plan<float>(*P) : build_plan<double>(*P);
+    if (rc != GPUFFT_SUCCESS) { plan_destroy(P); return rc; }
+    *out = P;
+    return GPUFFT_SUCCESS;
+}
+
+int plan_destroy(Plan *P) {
+    if (!P) return GPUFFT_SUCCESS;
+    if (P->tw_dev) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != P->device) cudaSetDevice(P->device);
+        cudaFree(P->tw_dev);
+        if (cur != P->device && cur >= 0) cudaSetDevice(cur);
+    }
+    delete P;
+    return GPUFFT_SUCCESS;
+}
+
+template <typename T>
+static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
+    PassAParams prm = P.pa;
+    prm.data = data;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(P.grid_a, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = P.smem_a;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = prm.K;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = fwd ? cudaLaunchKernelEx(&cfg, pass_a_kernel<T, true>, prm)
+                        : cudaLaunchKernelEx(&cfg, pass_a_kernel<T, false>, prm);
+    return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass A");
+}
+
+template <typename T>
+static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd) {
+    if (P.nx == 1) return GPUFFT_SUCCESS;  // a length-1 DFT is the identity
+    PassBParams prm = P.pb;
+    prm.data = data;
+    if (fwd)
+        pass_b_kernel<T, true><<<P.grid_b, kThreads, P.smem_b, s>>>(prm);
+    else
+        pass_b_kernel<T, false><<<P.grid_b, kThreads, P.smem_b, s>>>(prm);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass B");
+}
+
+int plan_exec(const Plan *P, void *data, void *stream, bool forward) {
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
+    if (((uintptr_t)data) % (P->dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
+        return set_error(GPUFFT_ERR_INVALID, "data pointer is not aligned to its complex type");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+    if (P->dtype == GPUFFT_FLOAT) {
+        if (forward) {
+            rc = launch_pass_a<float>(*P, data, s, true);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<float>(*P, data, s, true);
+        } else {
+            rc = launch_pass_b<float>(*P, data, s, false);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_a<float>(*P, data, s, false);
+        }
+    } else {
+        if (forward) {
+            rc = launch_pass_a<double>(*P, data, s, true);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<double>(*P, data, s, true);
+        } else {
+            rc = launch_pass_b<double>(*P, data, s, false);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_a<double>(*P, data, s, false);
+        }
+    }
+    return rc;
+}
+
+int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward) {
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
+    if (((uintptr_t)data) % (P->dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
+        return set_error(GPUFFT_ERR_INVALID, "data pointer is not aligned to its complex type");
+    if (pass != 0 && pass != 1) return set_error(GPUFFT_ERR_INVALID, "pass %d is neither 0 (A) nor 1 (B)", pass);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (P->dtype == GPUFFT_FLOAT)
+        return pass == 0 ? launch_pass_a<float>(*P, data, s, forward) : launch_pass_b<float>(*P, data, s, forward);
+    return pass == 0 ? launch_pass_a<double>(*P, data, s, forward) : launch_pass_b<double>(*P, data, s, forward);
+}
+
+int plan_launches(const Plan *P) { return P ? (P->nx == 1 ? 1 : 2) : 0; }
+
+static void describe_axis(std::string &out, const char *name, const AxisPlan &ax) {
+    char b[64];
+    snprintf(b, sizeof(b), "%s=%d[", name, ax.n);
+    out += b;
+    for (int s = 0; s < ax.nst; ++s) {
+        snprintf(b, sizeof(b), "%s%d", s ? "x" : "", ax.radix[s]);
+        out += b;
+    }
+    out += "]";
+}
+
+int plan_describe(const Plan *P, char *buf, int len) {
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    std::string s;
+    char b[256];
+    snprintf(b, sizeof(b), "grid=%lldx%lldx%lld dtype=%s ", (long long)P->nx, (long long)P->ny, (long long)P->nz,
+             P->dtype == GPUFFT_FLOAT ? "f32" : "f64");
+    s += b;
+    describe_axis(s, "x", P->pb.ax);
+    s += " ";
+    describe_axis(s, "y", P->pa.ay);
+    s += " ";
+    describe_axis(s, "zhalf", P->pa.az);
+    snprintf(b, sizeof(b),
+             " passA{K=%d grid=%d occ=%d smem=%zu wz=%d pz=%d wy=%d} passB{grid=%d occ=%d smem=%zu wx=%d tiles=%lld}",
+             P->pa.K, P->grid_a, P->occ_a, P->smem_a, P->pa.wz, P->pa.pz, P->pa.wy, P->grid_b, P->occ_b, P->smem_b,
+             P->pb.wx, P->pb.ntiles);
+    s += b;
+    if (buf && len > 0) {
+        strncpy(buf, s.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)s.size() + 1;
+}
+
+}  // namespace gpufft
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace gpufft;
+
+namespace {
+std::mutex g_mu;
+Plan *g_global[2] = {nullptr, nullptr};  // the reference-shaped singleton, one per dtype
+}  // namespace
+
+extern "C" int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank) {
+    if (procs != 1 || rank != 0)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "procs=%d rank=%d: only a size-1 communicator is supported", procs,
+                         rank);
+    Plan *P = nullptr;
+    const int rc = plan_create(&P, nx, ny, nz, dtype);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    std::lock_guard<std::mutex> lk(g_mu);
+    plan_destroy(g_global[dtype]);
+    g_global[dtype] = P;
+    return GPUFFT_SUCCESS;
+}
+
+static Plan *global_plan(int dtype) {
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_global[dtype];
+}
+
+extern "C" int gpufft_r2c(int dtype, void *data, void *stream) {
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return set_error(GPUFFT_ERR_INVALID, "bad dtype %d", dtype);
+    Plan *P = global_plan(dtype);
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "gpufft_r2c: no %s plan; call gpufft_init first",
+                             dtype == GPUFFT_FLOAT ? "float" : "double");
+    return plan_exec(P, data, stream, true);
+}
+
+extern "C" int gpufft_c2r(int dtype, void *data, void *stream) {
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return set_error(GPUFFT_ERR_INVALID, "bad dtype %d", dtype);
+    Plan *P = global_plan(dtype);
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "gpufft_c2r: no %s plan; call gpufft_init first",
+                             dtype == GPUFFT_FLOAT ? "float" : "double");
+    return plan_exec(P, data, stream, false);
+}
+
+extern "C" int gpufft_finalize(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto &p : g_global) {
+        plan_destroy(p);
+        p = nullptr;
+    }
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" const char *gpufft_last_error(void) { return last_error(); }
+
+extern "C" int gpufft_plan_create(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype) {
+    Plan *P = nullptr;
+    const int rc = plan_create(&P, nx, ny, nz, dtype);
+    if (plan) *plan = reinterpret_cast<gpufft_plan>(P);
+    return rc;
+}
+
+extern "C" int gpufft_plan_destroy(gpufft_plan plan) { return plan_destroy(reinterpret_cast<Plan *>(plan)); }
+
+extern "C" int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream) {
+    return plan_exec(reinterpret_cast<Plan *>(plan), data, stream, true);
+}
+
+extern "C" int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream) {
+    return plan_exec(reinterpret_cast<Plan *>(plan), data, stream, false);
+}
+
+extern "C" int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int forward) {
+    return plan_exec_pass(reinterpret_cast<Plan *>(plan), data, stream, pass, forward != 0);
+}
+
+extern "C" int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype) {
+    if (nx < 1 || ny < 1 || nz < 1 || (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE)) return -1;
+    return nx * ny * (nz / 2 + 1) * (dtype == GPUFFT_FLOAT ? 8 : 16);
+}
+
+extern "C" int gpufft_plan_launches(gpufft_plan plan) { return plan_launches(reinterpret_cast<Plan *>(plan)); }
+
+extern "C" int gpufft_plan_describe(gpufft_plan plan, char *buf, int len) {
+    return plan_describe(reinterpret_cast<Plan *>(plan), buf, len);
+}

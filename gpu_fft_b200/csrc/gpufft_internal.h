@@ -1,0 +1,32 @@
+// gpufft_internal.h — the plan object shared by the host translation units.
+#pragma once
+#include <cstdarg>
+#include <cstddef>
+#include <cstdint>
+
+#include "fft_kernels.cuh"
+
+namespace gpufft {
+
+struct Plan {
+    int64_t nx = 0, ny = 0, nz = 0;
+    int dtype = 0;
+    int device = 0;
+    void *tw_dev = nullptr;  // x, y, z twiddle tables back to back
+    PassAParams pa{};
+    PassBParams pb{};
+    size_t smem_a = 0, smem_b = 0;
+    int grid_a = 0, grid_b = 0;
+    int occ_a = 0, occ_b = 0;
+};
+
+int set_error(int code, const char *fmt, ...);
+const char *last_error();
+int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype);
+int plan_destroy(Plan *P);
+int plan_exec(const Plan *P, void *data, void *stream, bool forward);
+int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward);
+int plan_launches(const Plan *P);
+int plan_describe(const Plan *P, char *buf, int len);
+
+}  // namespace gpufft

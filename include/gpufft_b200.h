@@ -1,0 +1,108 @@
+/*
+ * gpufft_b200.h — C ABI of libgpufft_b200.so, the single-GPU, B200-native
+ * (sm_100a) replacement of GPU_FFT's 3D real-to-complex / complex-to-real
+ * transform.  Plain C types only: device pointers are void*, CUDA streams are
+ * passed as void* (a cudaStream_t; NULL = the legacy default stream).
+ *
+ * Data layout and semantics are the reference's at procs=1
+ * (GPU_FFT/src/GPU_FFT/GPU_FFT.h:111-121, Readme.md:47-52):
+ *  - real field: Nx x Ny x 2*(Nz/2+1) reals, row-major, each z-row padded by
+ *    2*(Nz/2+1)-Nz cells (GPU_FFT_TEST_SCRIPT/test.cu:124-135);
+ *  - spectrum, in place over the same bytes: Nx x Ny x (Nz/2+1) complex
+ *    (float2 / double2), kz fastest, ky, then kx — numpy.fft.rfftn's order;
+ *  - forward sign exp(-i...), no normalisation: c2r(r2c(f)) = Nx*Ny*Nz*f;
+ *  - c2r ignores the imaginary parts of bins kz=0 and kz=Nz/2 (even Nz), and
+ *    leaves the padding cells of every real row at zero.
+ * Both directions are asynchronous on the given stream (the reference returns
+ * with its last cuFFT launch in flight too, FFT_R2C.cu:69) and capturable in a
+ * CUDA graph: no host synchronisation, no allocation, no cuFFT.
+ *
+ * Every call returns a gpufft_status; gpufft_last_error() describes the most
+ * recent failure of the calling thread.  Nothing throws across the ABI.
+ */
+#ifndef GPUFFT_B200_H_
+#define GPUFFT_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GPUFFT_FLOAT = 0,  /* float  / cufftComplex       (TRANSITIONS::T1_f, T2_f) */
+    GPUFFT_DOUBLE = 1  /* double / cufftDoubleComplex (TRANSITIONS::T1_d, T2_d) */
+} gpufft_dtype;
+
+typedef enum {
+    GPUFFT_SUCCESS = 0,
+    GPUFFT_ERR_INVALID = 1,      /* bad argument (size < 1, null pointer, bad dtype) */
+    GPUFFT_ERR_UNSUPPORTED = 2,  /* valid but not handled (procs > 1, odd Nz, prime factor > 13, axis too long) */
+    GPUFFT_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+    GPUFFT_ERR_NOT_INIT = 4,     /* no plan for this dtype: call gpufft_init first */
+    GPUFFT_ERR_OOM = 5           /* device allocation failed */
+} gpufft_status;
+
+typedef struct gpufft_plan_s *gpufft_plan;
+
+/* --------------------------------------------------------------------------
+ * Reference-shaped entry points (one plan per dtype per process).
+ * ------------------------------------------------------------------------ */
+
+/* Replaces GPU_FFT::INIT_GPU_FFT<T1,T2>(Nx,Ny,Nz,procs,rank,comm)
+ * (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT_init.cu:41-93, with
+ * INIT_GPU_FFT_COMM, communications_setup.cu:56-71).  Builds (or rebuilds) the
+ * process-wide plan of `dtype` on the current CUDA device.  procs must be 1
+ * (rank 0); procs > 1 returns GPUFFT_ERR_UNSUPPORTED.  Unlike the reference,
+ * float and double plans coexist, re-initialising frees the previous plan,
+ * and no field-sized scratch buffer is allocated. */
+int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank);
+
+/* Replaces GPU_FFT::GPU_FFT_R2C<T1,T2>(T1*) (FFT_implementation/FFT_R2C.cu:41-70):
+ * in-place forward transform of `data` on `stream`. */
+int gpufft_r2c(int dtype, void *data, void *stream);
+
+/* Replaces GPU_FFT::GPU_FFT_C2R<T1,T2>(T2*) (FFT_implementation/FFT_C2R.cu:41-70):
+ * in-place inverse transform (unnormalised) of `data` on `stream`. */
+int gpufft_c2r(int dtype, void *data, void *stream);
+
+/* Frees the process-wide plans (the reference has no counterpart; its INIT
+ * leaks, GPU_FFT_init.cu:50,86-91). */
+int gpufft_finalize(void);
+
+/* Human-readable description of the calling thread's last error ("" if none). */
+const char *gpufft_last_error(void);
+
+/* --------------------------------------------------------------------------
+ * Plan objects: any number of grids / precisions per process.  The reference
+ * keeps one global plan (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT.cu:41-106);
+ * these are what the batched and serving layers build on.
+ * ------------------------------------------------------------------------ */
+int gpufft_plan_create(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype);
+int gpufft_plan_destroy(gpufft_plan plan);
+int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream);
+int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream);
+
+/* One of the two kernels of an exec, for per-kernel timing and for callers
+ * that fuse their own work between the passes.  pass 0 = Pass A (z and y
+ * axes, one x-plane per CTA cluster), pass 1 = Pass B (x axis).  A forward
+ * transform is pass 0 then pass 1; an inverse is pass 1 then pass 0.  (The
+ * reference's corresponding pieces are its cuFFT 2D R2C/C2R plan and its
+ * strided 1D C2C plan, GPU_FFT_init.cu:59-92.) */
+int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int forward);
+
+/* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
+int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);
+
+/* Kernel launches one exec issues (for launch accounting). */
+int gpufft_plan_launches(gpufft_plan plan);
+
+/* Text description of the plan (radices, tiles, cluster size), NUL-terminated
+ * into buf of size len; returns the full length needed. */
+int gpufft_plan_describe(gpufft_plan plan, char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUFFT_B200_H_ */
