@@ -15,8 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpufft_b200.so")
 
-SOURCES = ["gpufft.cu"]
-HEADERS = ["fft_kernels.cuh", "fft_radix.cuh", "gpufft_internal.h"]
+SOURCES = ["gpufft.cu", "fast_f32.cu", "fast_f64.cu"]
+HEADERS = ["fft_kernels.cuh", "fft_radix.cuh", "fft_fast.cuh", "fast_registry.h", "gpufft_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
@@ -40,14 +40,24 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile each source to an object in parallel, then link the library."""
     if not force and up_to_date():
         return LIB
-    srcs = [os.path.join(CSRC, f) for f in SOURCES]
-    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lcudart"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for f in SOURCES:
+        obj = os.path.join(objdir, f.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [nvcc(), *ARCH, *FLAGS, "-c", "-o", obj, os.path.join(CSRC, f)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd))
+        procs.append((f, subprocess.Popen(cmd)))
+    failed = [f for f, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed on {failed}")
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,41 @@
+// fast_registry.h — table of the compile-time specialised kernels.
+//
+// Each entry names one instantiation of fast::pass_a_fast / fast::pass_b_fast
+// (forward and inverse) with its shape parameters and shared-memory size.  The
+// plan looks up the entries matching its axis lengths; when several match it
+// either takes the first (the default) or, when autotuning, times them.
+#pragma once
+#include <cstddef>
+
+namespace gpufft {
+namespace fast {
+
+struct VariantA {
+    int dtype;       // GPUFFT_FLOAT / GPUFFT_DOUBLE
+    int ny, m;       // Ny and Nz/2
+    int wz, wy, nt;  // rows per row tile, columns per column tile, threads per CTA
+    int vy, vz;      // radix-list variants of the y and z/2 axes
+    size_t smem;     // dynamic shared memory per CTA
+    const void *kfwd, *kinv;
+};
+
+struct VariantB {
+    int dtype;
+    int nx;
+    int w, nt, v;
+    size_t smem;
+    const void *kfwd, *kinv;
+};
+
+// all entries of one precision (defined in fast_f32.cu / fast_f64.cu)
+extern const VariantA kVariantsA_f32[];
+extern const int kNumVariantsA_f32;
+extern const VariantB kVariantsB_f32[];
+extern const int kNumVariantsB_f32;
+extern const VariantA kVariantsA_f64[];
+extern const int kNumVariantsA_f64;
+extern const VariantB kVariantsB_f64[];
+extern const int kNumVariantsB_f64;
+
+}  // namespace fast
+}  // namespace gpufft

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -105,6 +106,101 @@ static int device_sms(int dev) {
     int v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
     return v > 0 ? v : 1;
+}
+
+// Cluster size for Pass A: enough CTAs per plane that the planes in flight
+// fit in about half of L2, and enough clusters to fill the GPU; at most 8
+// (the portable cluster limit) and at most one column tile per CTA.
+static int choose_cluster(int dev, int nx, int ny, int m, int wy, size_t plane_bytes, int occ, int sms) {
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    if (l2 <= 0) l2 = 96 << 20;
+    const int resident = std::max(1, occ) * sms;
+    const int tiles_y = (m + wy - 1) / wy;
+    const int kcap = std::max(1, std::min({8, tiles_y, ny}));
+    int K = 1;
+    while (K < kcap && (long long)(resident / K) * (long long)plane_bytes > (long long)l2 / 2) K *= 2;
+    while (K < kcap && (long long)nx * K < resident) K *= 2;
+    return std::min(K, kcap);
+}
+
+static int max_clusters(const void *kernel, int K, int nx, size_t smem, int nt, int fallback) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(K * std::max(1, nx), 1, 1);
+    cfg.blockDim = dim3(nt, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = K;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = fallback;
+    }
+    return n;
+}
+
+// Picks the specialised kernels for this plan's shape (first registry entry,
+// or the entries named by the autotuner) and sizes their launches.
+static int setup_fast(Plan &P, int idx_a, int idx_b) {
+    const int vs = P.dtype == GPUFFT_FLOAT ? 8 : 16;
+    const fast::VariantA *va = P.dtype == GPUFFT_FLOAT ? fast::kVariantsA_f32 : fast::kVariantsA_f64;
+    const int na = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsA_f32 : fast::kNumVariantsA_f64;
+    const fast::VariantB *vb = P.dtype == GPUFFT_FLOAT ? fast::kVariantsB_f32 : fast::kVariantsB_f64;
+    const int nb = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsB_f32 : fast::kNumVariantsB_f64;
+    const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
+    const int sms = device_sms(P.device);
+    P.fa = nullptr;
+    P.fb = nullptr;
+    int seen = 0;
+    for (int i = 0; i < na && !P.fa; ++i)
+        if (va[i].ny == ny && va[i].m == m && seen++ == idx_a) P.fa = &va[i];
+    seen = 0;
+    for (int i = 0; i < nb && !P.fb; ++i)
+        if (vb[i].nx == nx && seen++ == idx_b) P.fb = &vb[i];
+    if (P.fa) {
+        for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.fa->smem);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                P.fa = nullptr;
+                break;
+            }
+        }
+    }
+    if (P.fa) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, P.fa->kfwd, P.fa->nt, P.fa->smem);
+        P.occ_fa = std::max(occ, 1);
+        const size_t plane = (size_t)ny * (m + 1) * vs;
+        const int K = choose_cluster(P.device, nx, ny, m, P.fa->wy, plane, P.occ_fa, sms);
+        const int mc = max_clusters(P.fa->kfwd, K, nx, P.fa->smem, P.fa->nt, std::max(1, P.occ_fa * sms / K));
+        P.k_fa = K;
+        P.grid_fa = K * std::min(nx, mc);
+    }
+    if (P.fb) {
+        for (const void *k : {P.fb->kfwd, P.fb->kinv}) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.fb->smem);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                P.fb = nullptr;
+                break;
+            }
+        }
+    }
+    if (P.fb) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, P.fb->kfwd, P.fb->nt, P.fb->smem);
+        P.occ_fb = std::max(occ, 1);
+        const long long ncols = (long long)ny * (m + 1);
+        const long long tiles = (ncols + P.fb->w - 1) / P.fb->w;
+        P.grid_fb = (int)std::min<long long>(tiles, (long long)P.occ_fb * sms);
+    }
+    return GPUFFT_SUCCESS;
 }
 
 template <typename T>
@@ -202,42 +298,15 @@ static int build_plan(Plan &P) {
     occ_a = std::max(occ_a, 1);
     occ_b = std::max(occ_b, 1);
 
-    // Cluster size: enough CTAs per plane that the planes in flight fit in
-    // about half of L2, and enough clusters in total to fill the GPU; at most
-    // 8 (the portable cluster limit) and at most one column tile per CTA.
-    int l2 = 0;
-    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, P.device);
-    if (l2 <= 0) l2 = 96 << 20;
-    const long long plane_bytes = (long long)ny * nh * vs;
-    const int resident = occ_a * sms;
-    const int tiles_y = (m + wy - 1) / wy;
-    const int kcap = std::max(1, std::min({8, tiles_y, ny}));
-    int K = 1;
-    while (K < kcap && (long long)(resident / K) * plane_bytes > (long long)l2 / 2) K *= 2;
-    while (K < kcap && (long long)nx * K < resident) K *= 2;
-    K = std::min(K, kcap);
+    const size_t plane_bytes = (size_t)ny * nh * vs;
+    const int K = choose_cluster(P.device, nx, ny, m, wy, plane_bytes, occ_a, sms);
     A.K = K;
-
-    int max_clusters = 0;
-    {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        cfg.gridDim = dim3(K * std::max(1, nx), 1, 1);
-        cfg.blockDim = dim3(kThreads, 1, 1);
-        cfg.dynamicSmemBytes = P.smem_a;
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = K;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        e = cudaOccupancyMaxActiveClusters(&max_clusters, ka_f, &cfg);
-        if (e != cudaSuccess || max_clusters < 1) max_clusters = std::max(1, resident / K);
-    }
-    P.grid_a = K * std::min(nx, max_clusters);
+    const int max_cl = max_clusters((const void *)ka_f, K, nx, P.smem_a, kThreads, std::max(1, occ_a * sms / K));
+    P.grid_a = K * std::min(nx, max_cl);
     P.grid_b = (int)std::min<long long>(B.ntiles, (long long)occ_b * sms);
     P.occ_a = occ_a;
     P.occ_b = occ_b;
+    if (!std::getenv("GPUFFT_GENERIC_ONLY")) setup_fast(P, 0, 0);
     return GPUFFT_SUCCESS;
 }
 
@@ -281,6 +350,24 @@ template <typename T>
 static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
     PassAParams prm = P.pa;
     prm.data = data;
+    if (P.fa) {
+        prm.K = P.k_fa;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim = dim3(P.grid_fa, 1, 1);
+        cfg.blockDim = dim3(P.fa->nt, 1, 1);
+        cfg.dynamicSmemBytes = P.fa->smem;
+        cfg.stream = s;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = prm.K;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        void *args[] = {&prm};
+        const cudaError_t e = cudaLaunchKernelExC(&cfg, fwd ? P.fa->kfwd : P.fa->kinv, args);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass A (specialised)");
+    }
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     cfg.gridDim = dim3(P.grid_a, 1, 1);
@@ -303,6 +390,14 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd) {
     if (P.nx == 1) return GPUFFT_SUCCESS;  // a length-1 DFT is the identity
     PassBParams prm = P.pb;
     prm.data = data;
+    if (P.fb) {
+        prm.wx = P.fb->w;
+        prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
+        void *args[] = {&prm};
+        const cudaError_t e = cudaLaunchKernel(fwd ? P.fb->kfwd : P.fb->kinv, dim3(P.grid_fb), dim3(P.fb->nt), args,
+                                               P.fb->smem, s);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass B (specialised)");
+    }
     if (fwd)
         pass_b_kernel<T, true><<<P.grid_b, kThreads, P.smem_b, s>>>(prm);
     else
@@ -380,6 +475,16 @@ int plan_describe(const Plan *P, char *buf, int len) {
              P->pa.K, P->grid_a, P->occ_a, P->smem_a, P->pa.wz, P->pa.pz, P->pa.wy, P->grid_b, P->occ_b, P->smem_b,
              P->pb.wx, P->pb.ntiles);
     s += b;
+    if (P->fa) {
+        snprintf(b, sizeof(b), " fastA{ny=%d m=%d wz=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu}", P->fa->ny, P->fa->m,
+                 P->fa->wz, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa, P->fa->smem);
+        s += b;
+    }
+    if (P->fb) {
+        snprintf(b, sizeof(b), " fastB{nx=%d w=%d nt=%d v=%d grid=%d occ=%d smem=%zu}", P->fb->nx, P->fb->w,
+                 P->fb->nt, P->fb->v, P->grid_fb, P->occ_fb, P->fb->smem);
+        s += b;
+    }
     if (buf && len > 0) {
         strncpy(buf, s.c_str(), (size_t)len - 1);
         buf[len - 1] = 0;

@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "fast_registry.h"
 #include "fft_kernels.cuh"
 
 namespace gpufft {
@@ -18,6 +19,10 @@ struct Plan {
     size_t smem_a = 0, smem_b = 0;
     int grid_a = 0, grid_b = 0;
     int occ_a = 0, occ_b = 0;
+    // compile-time specialised kernels, when the registry has this shape
+    const fast::VariantA *fa = nullptr;
+    const fast::VariantB *fb = nullptr;
+    int grid_fa = 0, grid_fb = 0, k_fa = 1, occ_fa = 0, occ_fb = 0;
 };
 
 int set_error(int code, const char *fmt, ...);

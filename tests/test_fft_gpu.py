@@ -55,6 +55,9 @@ GRIDS = [
     (8, 8, 8), (16, 16, 16), (8, 6, 10), (12, 10, 14), (32, 24, 20), (64, 64, 64), (7, 9, 6), (5, 11, 26),
     (13, 13, 26), (1, 8, 8), (8, 1, 8), (8, 8, 2), (1, 1, 2), (3, 5, 4), (48, 40, 30), (96, 60, 50),
     (128, 32, 64), (32, 128, 16), (27, 25, 98), (64, 49, 44), (256, 16, 32), (16, 16, 512),
+    # shapes with compile-time specialised kernels (Pass A keyed on (Ny, Nz/2), Pass B on Nx)
+    (96, 96, 96), (128, 128, 128), (160, 160, 160), (192, 192, 192), (256, 256, 256), (256, 128, 64),
+    (512, 64, 64), (128, 512, 512),
 ]
 
 
@@ -277,3 +280,44 @@ def test_reference_test_program_against_this_library(cuda):
         assert abs(modes[k] - v / 128 ** 3) < 1e-6
     err = float(out.split("max error =")[1].split()[0])
     assert err < 1e-13
+
+
+@pytest.mark.parametrize("dt", ["float", "double"])
+def test_full_size_512_against_oracle(oracle, cuda, dt):
+    """512^3, the benchmark grid, against the FP64 C oracle on every output."""
+    n = 512
+    f = oracle.normal_field(n, n, n, seed=99, dtype=NPDT[dt])
+    want = oracle.c_r2c(f.astype(np.float64), n, n, n, steps=False)
+    got = run_r2c(f, (n, n, n), dt)
+    assert oracle.rel_l2(got, want) < TOL[dt]
+    back = run_c2r(want, (n, n, n), dt)
+    del got
+    want_back = oracle.c_c2r(want, n, n, n, steps=False)
+    assert oracle.rel_l2(back[:, :, :n], want_back[:, :, :n]) < TOL[dt]
+
+
+@pytest.mark.parametrize("grid", [(64, 64, 64), (128, 128, 128), (512, 512, 512), (256, 128, 64)], ids=str)
+def test_specialised_kernels_agree_with_generic(oracle, cuda, grid, monkeypatch):
+    """The compile-time specialised passes and the generic runtime-radix passes
+    compute the same transform (both within tolerance of the oracle, and within
+    a few float32 ulps of each other)."""
+    import torch
+    import gpu_fft_b200 as g
+
+    f = oracle.normal_field(*grid, seed=3, dtype=np.float32)
+    fast = g.Plan(*grid, "float")
+    monkeypatch.setenv("GPUFFT_GENERIC_ONLY", "1")
+    generic = g.Plan(*grid, "float")
+    monkeypatch.delenv("GPUFFT_GENERIC_ONLY")
+    assert "fastA" in fast.describe() or "fastB" in fast.describe()
+    assert "fastA" not in generic.describe() and "fastB" not in generic.describe()
+    a = torch.from_numpy(f.copy()).cuda()
+    b = a.clone()
+    fast.r2c(a)
+    generic.r2c(b)
+    torch.cuda.synchronize()
+    assert ((a - b).double().norm() / b.double().norm()).item() < 1e-6
+    fast.c2r(a)
+    generic.c2r(b)
+    torch.cuda.synchronize()
+    assert ((a - b).double().norm() / b.double().norm()).item() < 1e-6
