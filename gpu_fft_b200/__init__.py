@@ -28,7 +28,9 @@ EXPORTS = (
     "gpufft_init", "gpufft_r2c", "gpufft_c2r", "gpufft_finalize", "gpufft_last_error",
     "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_exec_r2c", "gpufft_exec_c2r",
     "gpufft_exec_pass", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
+    "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
 )
+GPUFFT_PLAN_AUTOTUNE = 1
 
 _lib = None
 
@@ -62,6 +64,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_field_bytes.restype = i64
     lib.gpufft_plan_launches.argtypes = [vp]
     lib.gpufft_plan_describe.argtypes = [vp, ctypes.c_char_p, ci]
+    lib.gpufft_plan_create_ex.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci, ci]
+    lib.gpufft_plan_autotune.argtypes = [vp, vp, vp]
+    lib.gpufft_wisdom_save.argtypes = [ctypes.c_char_p]
+    lib.gpufft_wisdom_load.argtypes = [ctypes.c_char_p]
     for name in EXPORTS:
         if getattr(lib, name, None) is None:
             raise ImportError(f"{path} does not export {name}")
@@ -107,13 +113,21 @@ def field_bytes(nx: int, ny: int, nz: int, dtype="float") -> int:
 class Plan:
     """A plan for one grid and precision (gpufft_plan_create)."""
 
-    def __init__(self, nx: int, ny: int, nz: int, dtype="float"):
+    def __init__(self, nx: int, ny: int, nz: int, dtype="float", autotune: bool = False):
         lib = load_library()
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dtype_code = _dtype_code(dtype)
         h = ctypes.c_void_p()
-        _check(lib.gpufft_plan_create(ctypes.byref(h), self.nx, self.ny, self.nz, self.dtype_code))
+        flags = GPUFFT_PLAN_AUTOTUNE if autotune else 0
+        _check(lib.gpufft_plan_create_ex(ctypes.byref(h), self.nx, self.ny, self.nz, self.dtype_code, flags))
         self._h = h
+
+    def autotune(self, scratch=None, stream=None) -> str:
+        """Time every compiled candidate of both passes (on `scratch`, a field-sized
+        CUDA tensor that gets overwritten, or a temporary buffer) and keep the fastest."""
+        ptr = scratch.data_ptr() if scratch is not None else None
+        _check(load_library().gpufft_plan_autotune(self._h, ptr, _stream_handle(stream) if stream is not None else None))
+        return self.describe()
 
     @property
     def handle(self) -> int:
@@ -202,6 +216,14 @@ def GPU_FFT_C2R(field, stream=None):
         raise ValueError("field must be a contiguous CUDA tensor")
     _check(load_library().gpufft_c2r(_field_dtype(field), field.data_ptr(), _stream_handle(stream)))
     return field
+
+
+def wisdom_save(path: str) -> None:
+    _check(load_library().gpufft_wisdom_save(path.encode()))
+
+
+def wisdom_load(path: str) -> None:
+    _check(load_library().gpufft_wisdom_load(path.encode()))
 
 
 def finalize() -> None:

@@ -1,40 +1,53 @@
 // fast_f32.cu — FP32 instantiations of the compile-time specialised passes.
 // Tile shapes: column tiles of 8 or 16 complex (64/128-byte rows), row tiles
-// of 16 rows, 256 threads per CTA; see fft_fast.cuh.
+// of whole rows per warp, 256 threads per CTA; see fft_fast.cuh.
 #include "fast_registry.h"
 #include "fft_fast.cuh"
 
 namespace gpufft {
 namespace fast {
 
-#define A_ENTRY(T, DT, NY, M, WZ, WY, NT, VY, VZ, MINB)                                                      \
-    {DT, NY, M, WZ, WY, NT, VY, VZ, PassAShape<T, NY, M, WZ, WY, NT, VY, VZ>::smem_bytes(),              \
-     (const void *)pass_a_fast<T, NY, M, WZ, WY, NT, true, VY, VZ, MINB>,                                     \
-     (const void *)pass_a_fast<T, NY, M, WZ, WY, NT, false, VY, VZ, MINB>}
+#define A_ENTRY(T, DT, NY, M, RW, WY, NT, VY, VZ, MINB)                                                      \
+    {0, 0, DT, NY, M, RW, WY, NT, VY, VZ, PassAShape<T, NY, M, RW, WY, NT, VY, VZ>::smem_bytes(),              \
+     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, true, VY, VZ, MINB>,                                     \
+     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, false, VY, VZ, MINB>}
+#define D_ENTRY(T, DT, NY, M, RW, WY, NT, K, VY, VZ, MINB)                                                   \
+    {1, K, DT, NY, M, RW, WY, NT, VY, VZ, PassADsmemShape<T, NY, M, RW, WY, NT, K, VY, VZ>::smem_bytes(),        \
+     (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, true, VY, VZ, MINB>,                                    \
+     (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, false, VY, VZ, MINB>}
+#define P_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
+    {1, DT, NX, W, NT, V, (size_t)(((NX + 1) / 2 * 2) + 2 * NX * W) * sizeof(cx_t<T>),                          \
+     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB>}
 #define B_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
-    {DT, NX, W, NT, V, (size_t)(NX + NX * W) * sizeof(cx_t<T>), (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB>, \
+    {0, DT, NX, W, NT, V, (size_t)(NX + NX * W) * sizeof(cx_t<T>), (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB>, \
      (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB>}
 
 const VariantA kVariantsA_f32[] = {
-    A_ENTRY(float, 0, 512, 256, 16, 8, 256, 0, 0, 3),
-    A_ENTRY(float, 0, 512, 256, 16, 16, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 512, 128, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 1024, 512, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 360, 240, 16, 8, 256, 0, 0, 1),
-    A_ENTRY(float, 0, 256, 128, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 192, 96, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 160, 80, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 128, 64, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 128, 32, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 96, 48, 16, 8, 256, 0, 0, 2),
-    A_ENTRY(float, 0, 64, 32, 16, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 512, 256, 2, 8, 256, 0, 0, 3),
+    A_ENTRY(float, 0, 512, 256, 2, 16, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 512, 256, 2, 8, 256, 0, 0, 4),
+    A_ENTRY(float, 0, 512, 256, 2, 8, 256, 1, 0, 3),
+    A_ENTRY(float, 0, 512, 128, 2, 8, 256, 0, 0, 2),
+    // plane held in the cluster's shared memory: correct, measured slower at 512^3
+    // (one 180 KB CTA per SM leaves 28 SMs idle); kept as an autotuning candidate
+    D_ENTRY(float, 0, 512, 256, 2, 8, 512, 8, 0, 0, 1),
+    A_ENTRY(float, 0, 1024, 512, 1, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 360, 240, 1, 8, 256, 0, 0, 1),
+    A_ENTRY(float, 0, 256, 128, 2, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 192, 96, 1, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 160, 80, 2, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 128, 64, 4, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 128, 32, 4, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 96, 48, 2, 8, 256, 0, 0, 2),
+    A_ENTRY(float, 0, 64, 32, 4, 8, 256, 0, 0, 2),
 };
 const int kNumVariantsA_f32 = sizeof(kVariantsA_f32) / sizeof(kVariantsA_f32[0]);
 
 const VariantB kVariantsB_f32[] = {
+    B_ENTRY(float, 0, 512, 16, 256, 1, 2),
     B_ENTRY(float, 0, 512, 16, 256, 0, 3),
     B_ENTRY(float, 0, 512, 8, 256, 0, 3),
-    B_ENTRY(float, 0, 512, 16, 256, 1, 2),
+    B_ENTRY(float, 0, 512, 16, 512, 1, 1),
     B_ENTRY(float, 0, 1024, 8, 256, 0, 2),
     B_ENTRY(float, 0, 384, 16, 256, 0, 2),
     B_ENTRY(float, 0, 256, 16, 256, 0, 2),

@@ -11,15 +11,19 @@ namespace gpufft {
 namespace fast {
 
 struct VariantA {
+    int kind;        // 0: plane exchanged through L2 (cluster size chosen at plan time)
+                     // 1: plane held in the cluster's shared memory (cluster size = k)
+    int k;           // cluster size of kind 1
     int dtype;       // GPUFFT_FLOAT / GPUFFT_DOUBLE
     int ny, m;       // Ny and Nz/2
-    int wz, wy, nt;  // rows per row tile, columns per column tile, threads per CTA
+    int rw, wy, nt;  // rows per warp in the row phase, columns per column tile, threads per CTA
     int vy, vz;      // radix-list variants of the y and z/2 axes
     size_t smem;     // dynamic shared memory per CTA
     const void *kfwd, *kinv;
 };
 
 struct VariantB {
+    int kind;  // 0: tiles loaded by the first FFT stage; 1: tiles double-buffered by cp.async
     int dtype;
     int nx;
     int w, nt, v;

@@ -69,6 +69,23 @@ __host__ __device__ constexpr int fac_prod(const Fac &f, int upto) {
     return p;
 }
 
+// Per-stage twiddle tables.  Stage s (radix R, sub-length p) uses
+// w_{pR}^{j*k} for j = 1..R-1, k = 0..p-1, stored at stage_offset(s) +
+// (j-1)*p + k: threads that hold consecutive k read consecutive entries
+// (conflict-free), and the stages together take sum (R_s - 1) p_s = N - 1
+// entries.  The host computes them in FP64 and rounds once.
+__host__ __device__ constexpr int stage_offset(const Fac &f, int s) {
+    int off = 0, p = 1;
+    for (int t = 0; t < s; ++t) {
+        off += (f.r[t] - 1) * p;
+        p *= f.r[t];
+    }
+    return off;
+}
+
+// which threads cooperate on a tile: the whole CTA, or one warp
+enum Scope { BLOCK = 0, WARP = 1 };
+
 // shared-memory layouts of a tile of W sequences of length N
 //  COLS: element (n, w) at n*W + w             (columns contiguous in w)
 //  ROWS: element (n, w) at w*PITCH + n + n/G   (one pad slot per G elements,
@@ -97,13 +114,27 @@ struct TileLayout {
 struct FromSmem {};
 struct ToSmem {};
 
-template <typename T, int N, int W, int NT, bool FWD, int LAYOUT, int TABMUL = 1, int VARIANT = 0>
+template <typename T, int N, int W, int NT, bool FWD, int LAYOUT, int VARIANT = 0, int SCOPE = BLOCK>
 struct TileFFT {
     using V = cx_t<T>;
     using L = TileLayout<T, N, W, LAYOUT>;
     static constexpr Fac F = factor(N, VARIANT);
     static constexpr int NS = F.n;
     static_assert(NS >= 0, "length must factor into 2,3,5,7,11,13");
+    static_assert(SCOPE == BLOCK || NT == 32, "a warp-scope tile has 32 threads");
+
+    static __device__ __forceinline__ void sync() {
+        if constexpr (SCOPE == WARP)
+            __syncwarp();
+        else
+            __syncthreads();
+    }
+    static __device__ __forceinline__ int tid() {
+        if constexpr (SCOPE == WARP)
+            return (int)(threadIdx.x & 31);
+        else
+            return (int)threadIdx.x;
+    }
 
     template <int S, class Src, class Dst>
     static __device__ __forceinline__ void stage(Src &src, Dst &dst, V *sm, const V *tw) {
@@ -116,10 +147,10 @@ struct TileFFT {
         constexpr bool last = (S == NS - 1);
         constexpr bool src_smem = !first || std::is_same<Src, FromSmem>::value;
         constexpr bool dst_smem = !last || std::is_same<Dst, ToSmem>::value;
-        const int tid = threadIdx.x;
+        const int tid = TileFFT::tid();
         V v[C][R];
         int ii[C], ww[C];
-        if (src_smem) __syncthreads();  // the previous writer of the tile is done
+        if (src_smem) sync();  // the previous writer of the tile is done
 #pragma unroll
         for (int m = 0; m < C; ++m) {
             const int q = tid + m * NT;
@@ -143,7 +174,7 @@ struct TileFFT {
                 }
             }
         }
-        if (dst_smem) __syncthreads();  // every reader of the tile is done before it is overwritten
+        if (dst_smem) sync();  // every reader of the tile is done before it is overwritten
 #pragma unroll
         for (int m = 0; m < C; ++m) {
             const int q = tid + m * NT;
@@ -151,9 +182,9 @@ struct TileFFT {
                 const int i = ii[m], w = ww[m];
                 const int k = i % p;
                 if constexpr (p > 1) {
-                    constexpr int step = TABMUL * (N / (p * R));
+                    constexpr int off = stage_offset(F, S);
 #pragma unroll
-                    for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tw[j * k * step]);
+                    for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tw[off + (j - 1) * p + k]);
                 }
                 Dft<R, FWD, V>::run(v[m]);
                 if constexpr (last) {
@@ -189,8 +220,8 @@ struct TileFFT {
     static __device__ __forceinline__ void run(Src &src, Dst &dst, V *sm, const V *tw) {
         if constexpr (NS == 0) {
             // length 1: identity (copy)
-            if constexpr (std::is_same<Src, FromSmem>::value) __syncthreads();
-            for (int q = threadIdx.x; q < W; q += NT) {
+            if constexpr (std::is_same<Src, FromSmem>::value) sync();
+            for (int q = tid(); q < W; q += NT) {
                 V x;
                 if constexpr (std::is_same<Src, FromSmem>::value) {
                     x = sm[L::idx(0, q)];
@@ -214,11 +245,11 @@ struct TileFFT {
 template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
     using V = cx_t<T>;
-    using FFT = TileFFT<T, NX, W, NT, FWD, COLS, 1, VARIANT>;
+    using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tw = reinterpret_cast<V *>(smem_raw);
     V *tile = tw + NX;
-    for (int q = threadIdx.x; q < NX; q += NT) tw[q] = reinterpret_cast<const V *>(P.twx)[q];
+    for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
     // (the first stage's barrier orders these writes before any twiddle read)
     V *base = reinterpret_cast<V *>(P.data);
     const long long ncols = P.ncols;
@@ -237,32 +268,121 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
 }
 
 // ---------------------------------------------------------------------------
-// Pass A: per x-plane z-axis R2C/C2R (rows) and y-axis C2C (columns)
+// Pass B with the tiles double-buffered by cp.async: while a tile is being
+// transformed (in place in shared memory, last stage written to global
+// memory), the next tile streams from global memory into the other buffer.
+// 16-byte copies; requires Ny*Nh even (row starts 16-byte aligned) and W even.
+// Columns of a ragged last tile past ncols are zero-filled by the copy.
 // ---------------------------------------------------------------------------
-template <typename T, int NY, int M, int WZ, int WY, int NT, int VY, int VZ>
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pass_b_pipe(PassBParams P) {
+    using V = cx_t<T>;
+    using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
+    constexpr int PER16 = 16 / (int)sizeof(V);  // complex per 16-byte chunk
+    constexpr int CH = W / PER16;                // chunks per tile row
+    static_assert(W % PER16 == 0, "tile rows must be whole 16-byte chunks");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *buf0 = tw + ((NX + PER16 - 1) / PER16) * PER16;
+    V *buf1 = buf0 + NX * W;
+    for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
+    const V *base = reinterpret_cast<const V *>(P.data);
+    V *obase = reinterpret_cast<V *>(P.data);
+    const long long ncols = P.ncols;
+    auto prefetch = [&](long long t, V *buf) {
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        for (int q = threadIdx.x; q < NX * CH; q += NT) {
+            const int n = q / CH, ch = q % CH;
+            const int w = ch * PER16;
+            const int valid = max(0, min(PER16, wv - w));
+            const V *src = base + (long long)n * ncols + c0 + (valid > 0 ? w : 0);
+            cp_async16(buf + n * W + w, src, valid * (int)sizeof(V));
+        }
+        cp_async_commit();
+    };
+    long long t = blockIdx.x;
+    if (t < P.ntiles) prefetch(t, buf0);
+    int k = 0;
+    for (; t < P.ntiles; t += gridDim.x, k ^= 1) {
+        V *cur = k ? buf1 : buf0;
+        V *nxt = k ? buf0 : buf1;
+        const long long tn = t + gridDim.x;
+        if (tn < P.ntiles) {
+            prefetch(tn, nxt);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        // (the FFT's first stage begins with a block barrier: the copies of
+        // every thread have landed before any thread reads the tile)
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        V *g = obase + c0;
+        auto dst = [&](int n, int w, V v) {
+            if (w < wv) st_g(g + (long long)n * ncols + w, v);
+        };
+        FromSmem fs;
+        FFT::run(fs, dst, cur, tw);
+        __syncthreads();  // the tile is free for the copy issued next iteration
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pass A: per x-plane z-axis R2C/C2R (rows, one warp per group of RW rows,
+// no CTA barrier) and y-axis C2C (column tiles of WY, whole CTA)
+// ---------------------------------------------------------------------------
+template <typename T, int NY, int M, int RW, int WY, int NT, int VY, int VZ>
 struct PassAShape {
     using V = cx_t<T>;
-    using RowL = TileLayout<T, M, WZ, ROWS>;
+    using RowL = TileLayout<T, M, RW, ROWS>;
     using ColL = TileLayout<T, NY, WY, COLS>;
-    static constexpr int TILE = RowL::ELEMS > ColL::ELEMS ? RowL::ELEMS : ColL::ELEMS;
-    static constexpr size_t smem_bytes() { return (size_t)(2 * M + NY + TILE) * sizeof(V); }
+    static constexpr int NWARP = NT / 32;
+    static constexpr int ROWS_ELEMS = NWARP * RowL::ELEMS;
+    static constexpr int TILE = ROWS_ELEMS > ColL::ELEMS ? ROWS_ELEMS : ColL::ELEMS;
+    // unpack roots w_Nz^k (k <= M/2), z and y stage tables, tile
+    static constexpr int UNP = M / 2 + 1;
+    static constexpr size_t smem_bytes() { return (size_t)(UNP + M + NY + TILE) * sizeof(V); }
 };
 
-template <typename T, int NY, int M, int WZ, int WY, int NT, bool FWD, int VY, int VZ, int MINB>
+// Split cluster barrier: arrive (release) after a phase, wait (acquire)
+// before the dependent phase; the CTA may do independent work in between.
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB>
 __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     using V = cx_t<T>;
-    using Shape = PassAShape<T, NY, M, WZ, WY, NT, VY, VZ>;
-    using RowFFT = TileFFT<T, M, WZ, NT, FWD, ROWS, 2, VZ>;
-    using ColFFT = TileFFT<T, NY, WY, NT, FWD, COLS, 1, VY>;
+    using Shape = PassAShape<T, NY, M, RW, WY, NT, VY, VZ>;
+    using RowFFT = TileFFT<T, M, RW, 32, FWD, ROWS, VZ, WARP>;
+    using ColFFT = TileFFT<T, NY, WY, NT, FWD, COLS, VY, BLOCK>;
     using RowL = typename RowFFT::L;
     using ColL = typename ColFFT::L;
-    constexpr int NZ = 2 * M, NH = M + 1;
+    constexpr int NH = M + 1;
+    constexpr int UNP = Shape::UNP;
+    constexpr int HALF = M / 2 + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *twz = reinterpret_cast<V *>(smem_raw);
-    V *twy = twz + NZ;
-    V *tile = twy + NY;
-    for (int q = threadIdx.x; q < NZ; q += NT) twz[q] = reinterpret_cast<const V *>(P.twz)[q];
-    for (int q = threadIdx.x; q < NY; q += NT) twy[q] = reinterpret_cast<const V *>(P.twy)[q];
+    V *unp = reinterpret_cast<V *>(smem_raw);
+    V *stz = unp + UNP;
+    V *sty = stz + M;
+    V *tile = sty + NY;
+    for (int q = threadIdx.x; q < UNP; q += NT) unp[q] = reinterpret_cast<const V *>(P.twz)[q];
+    for (int q = threadIdx.x; q < M - 1; q += NT) stz[q] = reinterpret_cast<const V *>(P.stz)[q];
+    for (int q = threadIdx.x; q < NY - 1; q += NT) sty[q] = reinterpret_cast<const V *>(P.sty)[q];
     __syncthreads();
 
     const int K = P.K;
@@ -272,50 +392,296 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     const int rows_per = (NY + K - 1) / K;
     const int rb = min(NY, crank * rows_per), re = min(NY, rb + rows_per);
     constexpr int ntiles_y = (M + WY - 1) / WY;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    V *wtile = tile + wid * RowL::ELEMS;  // this warp's rows (overlaps the column tile)
     V *base = reinterpret_cast<V *>(P.data);
     const T hf = (T)0.5;
 
+    // ---------------- y columns of plane g (whole CTA) ----------------
+    auto cols = [&](V *g) {
+        for (int t = crank; t < ntiles_y; t += K) {
+            const int c0 = t * WY;
+            const int wv = min(WY, M - c0);
+            V *gc = g + c0;
+            auto src = [&](int n, int w) -> V {
+                return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
+            };
+            auto dst = [&](int n, int w, V v) {
+                if (w < wv) st_g(gc + (long long)n * NH + w, v);
+            };
+            if (c0 != 0) {
+                ColFFT::run(src, dst, tile, sty);
+            } else if (FWD) {
+                // column 0 carries (bin 0) + i (bin m); split after the FFT
+                ToSmem ts;
+                ColFFT::run(src, ts, tile, sty);
+                __syncthreads();
+                for (int q = threadIdx.x; q < NY * WY; q += NT) {
+                    const int n = q / WY, w = q % WY;
+                    if (w >= wv) continue;
+                    const V c1 = tile[ColL::idx(n, w)];
+                    if (w == 0) {
+                        const V c2 = c_conj(tile[ColL::idx((NY - n) % NY, 0)]);
+                        st_g(g + (long long)n * NH, c_scale(c_add(c1, c2), hf));
+                        st_g(g + (long long)n * NH + M, c_rot<true>(c_scale(c_sub(c1, c2), hf)));
+                    } else {
+                        st_g(gc + (long long)n * NH + w, c1);
+                    }
+                }
+            } else {
+                // inverse: Hermitian projection of bins kz=0 (a) and kz=m (b) along y,
+                // packed as a' + i b' into column 0 in place (each thread owns the
+                // pair of rows n, -n), then the plain column FFT
+                __syncthreads();
+                for (int n = threadIdx.x; n <= NY / 2; n += NT) {
+                    const int n2 = (NY - n) % NY;
+                    const V a1 = ld_g(g + (long long)n * NH), a2 = ld_g(g + (long long)n2 * NH);
+                    const V b1 = ld_g(g + (long long)n * NH + M), b2 = ld_g(g + (long long)n2 * NH + M);
+                    const V ha = c_scale(c_add(a1, c_conj(a2)), hf);
+                    const V hb = c_scale(c_add(b1, c_conj(b2)), hf);
+                    st_g(g + (long long)n * NH, V{ha.x - hb.y, ha.y + hb.x});
+                    if (n2 != n) st_g(g + (long long)n2 * NH, V{ha.x + hb.y, -ha.y + hb.x});
+                }
+                __syncthreads();
+                ColFFT::run(src, dst, tile, sty);
+            }
+        }
+    };
+    // ---------------- z rows of plane g: each warp takes RW rows at a time ----------------
+    auto rows = [&](V *g) {
+        for (int r0 = rb + wid * RW; r0 < re; r0 += (NT / 32) * RW) {
+            const int wv = min(RW, re - r0);
+            V *gr = g + (long long)r0 * NH;
+            if (FWD) {
+                auto src = [&](int n, int w) -> V {
+                    return (w < wv) ? ld_g(gr + (long long)w * NH + n) : V{(T)0, (T)0};
+                };
+                ToSmem ts;
+                RowFFT::run(src, ts, wtile, stz);
+                __syncwarp();
+                // unpack: X[k] = E + O, X[m-k] = conj(E - O), E = (Z[k] + conj Z[m-k])/2,
+                // O = -i w^k (Z[k] - conj Z[m-k])/2, w = exp(-2 pi i/Nz); bins 0 and m packed in slot 0
+                for (int w = 0; w < wv; ++w) {
+                    V *row = gr + (long long)w * NH;
+                    for (int k = lane; k < HALF; k += 32) {
+                        const V a = wtile[RowL::idx(k, w)];
+                        const V b = c_conj(wtile[RowL::idx(k == 0 ? 0 : M - k, w)]);
+                        const V e = c_scale(c_add(a, b), hf);
+                        const V d = c_scale(c_sub(a, b), hf);
+                        const V o = c_rot<true>(c_mul(d, unp[k]));
+                        const V xa = c_add(e, o), xb = c_conj(c_sub(e, o));
+                        if (k == 0) {
+                            st_g(row, V{xa.x, xb.x});
+                        } else {
+                            st_g(row + k, xa);
+                            if (M - k != k) st_g(row + M - k, xb);
+                        }
+                    }
+                }
+            } else {
+                // pre-process: Z[k] = S + Pk, Z[m-k] = conj(S - Pk), S = X[k] + conj X[m-k],
+                // Pk = i conj(w^k)(X[k] - conj X[m-k]); slot 0 holds (Re X0, Re Xm)
+                __syncwarp();
+                for (int w = 0; w < RW; ++w) {
+                    const V *row = gr + (long long)w * NH;
+                    for (int k = lane; k < HALF; k += 32) {
+                        V za = V{(T)0, (T)0}, zb = V{(T)0, (T)0};
+                        if (w < wv) {
+                            V xk, xmk;
+                            if (k == 0) {
+                                const V pk = ld_g(row);
+                                xk = V{pk.x, (T)0};
+                                xmk = V{pk.y, (T)0};
+                            } else {
+                                xk = ld_g(row + k);
+                                xmk = ld_g(row + M - k);
+                            }
+                            const V cm = c_conj(xmk);
+                            const V s = c_add(xk, cm);
+                            const V pk = c_rot<false>(c_mulc(c_sub(xk, cm), unp[k]));
+                            za = c_add(s, pk);
+                            zb = c_conj(c_sub(s, pk));
+                        }
+                        wtile[RowL::idx(k, w)] = za;
+                        if (k != 0 && M - k != k) wtile[RowL::idx(M - k, w)] = zb;
+                    }
+                }
+                auto dst = [&](int n, int w, V v) {
+                    if (w < wv) st_g(gr + (long long)w * NH + n, v);
+                };
+                FromSmem fs;
+                RowFFT::run(fs, dst, wtile, stz);
+                // slot m = padding cells of the real row: zero
+                if (lane < wv) st_g(gr + (long long)lane * NH + M, V{(T)0, (T)0});
+            }
+        }
+    };
+
+    // Schedule: forward runs rows then columns of each plane, inverse the
+    // reverse, with the cluster barrier (release/acquire, so the plane's
+    // rows written by every CTA of the cluster are visible) in between.
+    // Running the next plane's first phase before the barrier wait was
+    // measured slower at 512^3: two planes per cluster in flight overflow L2.
+    // Block barriers separate the warp-private row tiles from the shared
+    // column tile, which overlap in shared memory.
     for (int plane = cid; plane < P.nx; plane += ncl) {
         V *g = base + (long long)plane * NY * NH;
-        // ---------------- y columns (inverse: first) ----------------
-        auto cols = [&](auto fwd_tag) {
-            constexpr bool F = decltype(fwd_tag)::value;
+        if (FWD)
+            rows(g);
+        else
+            cols(g);
+        __syncthreads();
+        if (K > 1) {
+            cluster_arrive();
+            cluster_wait();
+        }
+        if (FWD)
+            cols(g);
+        else
+            rows(g);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pass A, distributed-shared-memory form.  A cluster of K CTAs holds one
+// x-plane in shared memory: CTA r owns rows [r*NY/K, (r+1)*NY/K) of the
+// plane (ROWS layout, its "slice").  Forward: every warp transforms its rows
+// from global memory in place in the slice (z R2C + unpack); cluster barrier;
+// the column tiles read the slices of all CTAs of the cluster over DSMEM, run
+// the y FFT and write the result to global memory; cluster barrier before the
+// next plane overwrites the slices.  Inverse: the y inverse writes its output
+// into the owners' slices over DSMEM, then each warp runs the z C2R of its
+// rows from the slice to global memory.  Global memory sees one read and one
+// write of the field; no L2 round trip between the axes.
+// ---------------------------------------------------------------------------
+template <typename T, int NY, int M, int RW, int WY, int NT, int K, int VY, int VZ>
+struct PassADsmemShape {
+    using V = cx_t<T>;
+    using SliceL = TileLayout<T, M, NY / K, ROWS>;
+    using ColL = TileLayout<T, NY, WY, COLS>;
+    static constexpr int UNP = M / 2 + 1;
+    static constexpr size_t smem_bytes() {
+        return (size_t)(UNP + M + NY + SliceL::ELEMS + ColL::ELEMS) * sizeof(V);
+    }
+};
+
+template <typename T, int NY, int M, int RW, int WY, int NT, int K, bool FWD, int VY, int VZ, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pass_a_dsmem(PassAParams P) {
+    using V = cx_t<T>;
+    using Shape = PassADsmemShape<T, NY, M, RW, WY, NT, K, VY, VZ>;
+    constexpr int SLICE = NY / K;
+    static_assert(NY % K == 0, "rows must split evenly over the cluster");
+    static_assert(SLICE % RW == 0, "warp row groups must tile the slice");
+    using RowFFT = TileFFT<T, M, RW, 32, FWD, ROWS, VZ, WARP>;
+    using ColFFT = TileFFT<T, NY, WY, NT, FWD, COLS, VY, BLOCK>;
+    using SliceL = typename Shape::SliceL;
+    using ColL = typename ColFFT::L;
+    static_assert(SliceL::PITCH == RowFFT::L::PITCH, "row tiles live inside the slice");
+    constexpr int NH = M + 1;
+    constexpr int UNP = Shape::UNP;
+    constexpr int HALF = M / 2 + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *unp = reinterpret_cast<V *>(smem_raw);
+    V *stz = unp + UNP;
+    V *sty = stz + M;
+    V *slice = sty + NY;
+    V *ctile = slice + SliceL::ELEMS;
+    for (int q = threadIdx.x; q < UNP; q += NT) unp[q] = reinterpret_cast<const V *>(P.twz)[q];
+    for (int q = threadIdx.x; q < M - 1; q += NT) stz[q] = reinterpret_cast<const V *>(P.stz)[q];
+    for (int q = threadIdx.x; q < NY - 1; q += NT) sty[q] = reinterpret_cast<const V *>(P.sty)[q];
+    __syncthreads();
+
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int cid = blockIdx.x / K;
+    const int ncl = gridDim.x / K;
+    constexpr int ntiles_y = (M + WY - 1) / WY;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    V *base = reinterpret_cast<V *>(P.data);
+    const T hf = (T)0.5;
+    // element (row n, column c) of the plane in the owner's slice (DSMEM address)
+    auto at = [&](int n, int c) -> V * {
+        return cluster.map_shared_rank(slice + SliceL::idx(c, n % SLICE), n / SLICE);
+    };
+
+    for (int plane = cid; plane < P.nx; plane += ncl) {
+        V *g = base + (long long)plane * NY * NH;
+        V *gs = g + (long long)crank * SLICE * NH;  // this CTA's rows in global memory
+        if (FWD) {
+            // ---- z rows: global -> slice, R2C, unpack in place ----
+            for (int lr = wid * RW; lr < SLICE; lr += (NT / 32) * RW) {
+                V *gr = gs + (long long)lr * NH;
+                V *wt = slice + lr * SliceL::PITCH;
+                auto src = [&](int n, int w) -> V { return ld_g(gr + (long long)w * NH + n); };
+                ToSmem ts;
+                RowFFT::run(src, ts, wt, stz);
+                __syncwarp();
+                for (int w = 0; w < RW; ++w) {
+                    for (int k = lane; k < HALF; k += 32) {
+                        const int km = (k == 0) ? 0 : M - k;
+                        const V a = wt[SliceL::idx(k, w)];
+                        const V b = c_conj(wt[SliceL::idx(km, w)]);
+                        const V e = c_scale(c_add(a, b), hf);
+                        const V d = c_scale(c_sub(a, b), hf);
+                        const V o = c_rot<true>(c_mul(d, unp[k]));
+                        const V xa = c_add(e, o), xb = c_conj(c_sub(e, o));
+                        if (k == 0) {
+                            wt[SliceL::idx(0, w)] = V{xa.x, xb.x};
+                        } else {
+                            wt[SliceL::idx(k, w)] = xa;
+                            if (km != k) wt[SliceL::idx(km, w)] = xb;
+                        }
+                    }
+                }
+            }
+            cluster.sync();
+            // ---- y columns: slices (DSMEM) -> y FFT -> global ----
             for (int t = crank; t < ntiles_y; t += K) {
                 const int c0 = t * WY;
                 const int wv = min(WY, M - c0);
                 V *gc = g + c0;
+                auto src = [&](int n, int w) -> V { return (w < wv) ? *at(n, c0 + w) : V{(T)0, (T)0}; };
                 auto dst = [&](int n, int w, V v) {
                     if (w < wv) st_g(gc + (long long)n * NH + w, v);
                 };
                 if (c0 != 0) {
-                    auto src = [&](int n, int w) -> V {
-                        return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
-                    };
-                    ColFFT::run(src, dst, tile, twy);
-                } else if (F) {
-                    // column 0 carries (bin 0) + i (bin m); split after the FFT
-                    auto src = [&](int n, int w) -> V {
-                        return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
-                    };
+                    ColFFT::run(src, dst, ctile, sty);
+                } else {
                     ToSmem ts;
-                    ColFFT::run(src, ts, tile, twy);
+                    ColFFT::run(src, ts, ctile, sty);
                     __syncthreads();
                     for (int q = threadIdx.x; q < NY * WY; q += NT) {
                         const int n = q / WY, w = q % WY;
                         if (w >= wv) continue;
-                        const V c1 = tile[ColL::idx(n, w)];
+                        const V c1 = ctile[ColL::idx(n, w)];
                         if (w == 0) {
-                            const V c2 = c_conj(tile[ColL::idx((NY - n) % NY, 0)]);
+                            const V c2 = c_conj(ctile[ColL::idx((NY - n) % NY, 0)]);
                             st_g(g + (long long)n * NH, c_scale(c_add(c1, c2), hf));
                             st_g(g + (long long)n * NH + M, c_rot<true>(c_scale(c_sub(c1, c2), hf)));
                         } else {
                             st_g(gc + (long long)n * NH + w, c1);
                         }
                     }
-                } else {
-                    // inverse: Hermitian projection of bins kz=0 (a) and kz=m (b) along y,
-                    // packed as a' + i b' into column 0 in place (each thread owns the
-                    // pair of rows n, -n), then the plain column FFT
+                }
+            }
+            cluster.sync();  // every peer is done reading the slices
+        } else {
+            // ---- y columns: global -> y inverse FFT -> owners' slices (DSMEM) ----
+            for (int t = crank; t < ntiles_y; t += K) {
+                const int c0 = t * WY;
+                const int wv = min(WY, M - c0);
+                V *gc = g + c0;
+                auto src = [&](int n, int w) -> V {
+                    return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
+                };
+                auto dst = [&](int n, int w, V v) {
+                    if (w < wv) *at(n, c0 + w) = v;
+                };
+                if (c0 == 0) {
+                    // Hermitian projection of bins kz=0 and kz=m along y, packed into column 0
+                    __syncthreads();
                     for (int n = threadIdx.x; n <= NY / 2; n += NT) {
                         const int n2 = (NY - n) % NY;
                         const V a1 = ld_g(g + (long long)n * NH), a2 = ld_g(g + (long long)n2 * NH);
@@ -326,94 +692,39 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
                         if (n2 != n) st_g(g + (long long)n2 * NH, V{ha.x + hb.y, -ha.y + hb.x});
                     }
                     __syncthreads();
-                    auto src = [&](int n, int w) -> V {
-                        return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
-                    };
-                    ColFFT::run(src, dst, tile, twy);
                 }
+                ColFFT::run(src, dst, ctile, sty);
             }
-        };
-        // ---------------- z rows ----------------
-        auto rows_fwd = [&]() {
-            for (int r0 = rb; r0 < re; r0 += WZ) {
-                const int wv = min(WZ, re - r0);
-                V *gr = g + (long long)r0 * NH;
-                auto src = [&](int n, int w) -> V {
-                    return (w < wv) ? ld_g(gr + (long long)w * NH + n) : V{(T)0, (T)0};
-                };
-                ToSmem ts;
-                RowFFT::run(src, ts, tile, twz);
-                __syncthreads();
-                // unpack: X[k] = E + O, X[m-k] = conj(E - O), E = (Z[k] + conj Z[m-k])/2,
-                // O = -i w^k (Z[k] - conj Z[m-k])/2, w = exp(-2 pi i/Nz); bins 0 and m packed in slot 0
-                constexpr int HALF = M / 2 + 1;
-                for (int q = threadIdx.x; q < HALF * WZ; q += NT) {
-                    const int k = q % HALF, w = q / HALF;
-                    if (w >= wv) continue;
-                    const V a = tile[RowL::idx(k, w)];
-                    const V b = c_conj(tile[RowL::idx(k == 0 ? 0 : M - k, w)]);
-                    const V e = c_scale(c_add(a, b), hf);
-                    const V d = c_scale(c_sub(a, b), hf);
-                    const V o = c_rot<true>(c_mul(d, twz[k]));
-                    const V xa = c_add(e, o), xb = c_conj(c_sub(e, o));
-                    V *row = gr + (long long)w * NH;
-                    if (k == 0) {
-                        st_g(row, V{xa.x, xb.x});
-                    } else {
-                        st_g(row + k, xa);
-                        if (M - k != k) st_g(row + M - k, xb);
-                    }
-                }
-            }
-        };
-        auto rows_inv = [&]() {
-            for (int r0 = rb; r0 < re; r0 += WZ) {
-                const int wv = min(WZ, re - r0);
-                V *gr = g + (long long)r0 * NH;
-                // pre-process: Z[k] = S + Pk, Z[m-k] = conj(S - Pk), S = X[k] + conj X[m-k],
-                // Pk = i conj(w^k)(X[k] - conj X[m-k]); slot 0 holds (Re X0, Re Xm)
-                constexpr int HALF = M / 2 + 1;
-                __syncthreads();
-                for (int q = threadIdx.x; q < HALF * WZ; q += NT) {
-                    const int k = q % HALF, w = q / HALF;
-                    V za = V{(T)0, (T)0}, zb = V{(T)0, (T)0};
-                    if (w < wv) {
-                        const V *row = gr + (long long)w * NH;
+            cluster.sync();
+            // ---- z rows: slice -> pre-process -> C2R -> global ----
+            for (int lr = wid * RW; lr < SLICE; lr += (NT / 32) * RW) {
+                V *gr = gs + (long long)lr * NH;
+                V *wt = slice + lr * SliceL::PITCH;
+                for (int w = 0; w < RW; ++w) {
+                    for (int k = lane; k < HALF; k += 32) {
+                        const int km = M - k;
                         V xk, xmk;
                         if (k == 0) {
-                            const V pk = ld_g(row);
+                            const V pk = wt[SliceL::idx(0, w)];
                             xk = V{pk.x, (T)0};
                             xmk = V{pk.y, (T)0};
                         } else {
-                            xk = ld_g(row + k);
-                            xmk = ld_g(row + M - k);
+                            xk = wt[SliceL::idx(k, w)];
+                            xmk = wt[SliceL::idx(km, w)];
                         }
                         const V cm = c_conj(xmk);
-                        const V s = c_add(xk, cm);
-                        const V pk = c_rot<false>(c_mulc(c_sub(xk, cm), twz[k]));
-                        za = c_add(s, pk);
-                        zb = c_conj(c_sub(s, pk));
+                        const V sv = c_add(xk, cm);
+                        const V pk = c_rot<false>(c_mulc(c_sub(xk, cm), unp[k]));
+                        wt[SliceL::idx(k, w)] = c_add(sv, pk);
+                        if (k != 0 && km != k) wt[SliceL::idx(km, w)] = c_conj(c_sub(sv, pk));
                     }
-                    tile[RowL::idx(k, w)] = za;
-                    if (k != 0 && M - k != k) tile[RowL::idx(M - k, w)] = zb;
                 }
-                auto dst = [&](int n, int w, V v) {
-                    if (w < wv) st_g(gr + (long long)w * NH + n, v);
-                };
+                auto dst = [&](int n, int w, V v) { st_g(gr + (long long)w * NH + n, v); };
                 FromSmem fs;
-                RowFFT::run(fs, dst, tile, twz);
-                // slot m = padding cells of the real row: zero
-                for (int q = threadIdx.x; q < wv; q += NT) st_g(gr + (long long)q * NH + M, V{(T)0, (T)0});
+                RowFFT::run(fs, dst, wt, stz);
+                if (lane < RW) st_g(gr + (long long)lane * NH + M, V{(T)0, (T)0});
             }
-        };
-        if (FWD) {
-            rows_fwd();
-            cluster_barrier(K);
-            cols(std::integral_constant<bool, true>{});
-        } else {
-            cols(std::integral_constant<bool, false>{});
-            cluster_barrier(K);
-            rows_inv();
+            cluster.sync();  // slices free for the next plane's columns
         }
     }
 }

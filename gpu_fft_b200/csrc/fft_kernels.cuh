@@ -55,6 +55,8 @@ struct PassAParams {
     void *data;          // field base (complex view)
     const void *twz;     // exp(-2 pi i e / Nz), e < Nz
     const void *twy;     // exp(-2 pi i e / Ny), e < Ny
+    const void *stz;     // per-stage tables of the specialised kernels (fft_fast.cuh)
+    const void *sty;
     int nx, ny, nz, nh, m;  // m = Nz/2
     int K;               // CTAs per cluster (per x-plane)
     // phase with rows (z axis): tile of wz rows, smem row pitch pz (odd)
@@ -71,6 +73,7 @@ struct PassAParams {
 struct PassBParams {
     void *data;
     const void *twx;
+    const void *stw;     // per-stage table of the specialised kernel (fft_fast.cuh)
     int nx;
     long long ncols;   // Ny * Nh
     int wx;

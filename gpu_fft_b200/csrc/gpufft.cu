@@ -13,12 +13,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/gpufft_b200.h"
+#include "fft_fast.cuh"
 #include "fft_kernels.cuh"
 #include "gpufft_internal.h"
 
@@ -99,6 +104,58 @@ static std::vector<T> twiddle_table(int L) {
     return t;
 }
 
+// Per-stage table of the specialised kernels for length n (fft_fast.cuh,
+// stage_offset): stage s with radix R after sub-length p holds
+// exp(-2 pi i j k / (p R)) at offset + (j-1)*p + k.  Padded to n entries.
+template <typename T>
+static std::vector<T> stage_table(int n, int variant) {
+    const fast::Fac f = fast::factor(n, variant);
+    std::vector<T> t(2 * (size_t)std::max(n, 1), (T)0);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    int p = 1;
+    for (int s = 0; s < f.n; ++s) {
+        const int R = f.r[s], off = fast::stage_offset(f, s);
+        for (int j = 1; j < R; ++j)
+            for (int k = 0; k < p; ++k) {
+                const long long e = ((long long)j * k) % ((long long)p * R);
+                const long double ang = two_pi * (long double)e / (long double)(p * R);
+                const size_t at = (size_t)off + (size_t)(j - 1) * p + k;
+                t[2 * at] = (T)cosl(ang);
+                t[2 * at + 1] = (T)(-sinl(ang));
+            }
+        p *= R;
+    }
+    return t;
+}
+
+template <typename T>
+static int upload_stage_tables(Plan &P) {
+    const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
+    std::vector<T> tx, ty, tz;
+    if (P.fb) tx = stage_table<T>(nx, P.fb->v);
+    if (P.fa) {
+        ty = stage_table<T>(ny, P.fa->vy);
+        tz = stage_table<T>(m, P.fa->vz);
+    }
+    const size_t bx = tx.size() * sizeof(T), by = ty.size() * sizeof(T), bz = tz.size() * sizeof(T);
+    if (P.stage_dev) {
+        cudaFree(P.stage_dev);
+        P.stage_dev = nullptr;
+    }
+    if (bx + by + bz == 0) return GPUFFT_SUCCESS;
+    cudaError_t e = cudaMalloc(&P.stage_dev, bx + by + bz);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_OOM, "cudaMalloc stage tables: %s", cudaGetErrorString(e));
+    char *b = (char *)P.stage_dev;
+    if (bx) e = cudaMemcpy(b, tx.data(), bx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && by) e = cudaMemcpy(b + bx, ty.data(), by, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && bz) e = cudaMemcpy(b + bx + by, tz.data(), bz, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpy stage tables");
+    P.pb.stw = bx ? b : nullptr;
+    P.pa.sty = by ? b + bx : nullptr;
+    P.pa.stz = bz ? b + bx + by : nullptr;
+    return GPUFFT_SUCCESS;
+}
+
 // ---------------------------------------------------------------------------
 // plan
 // ---------------------------------------------------------------------------
@@ -156,12 +213,15 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
     const int sms = device_sms(P.device);
     P.fa = nullptr;
     P.fb = nullptr;
+    P.idx_a = idx_a;
+    P.idx_b = idx_b;
     int seen = 0;
     for (int i = 0; i < na && !P.fa; ++i)
         if (va[i].ny == ny && va[i].m == m && seen++ == idx_a) P.fa = &va[i];
     seen = 0;
+    const bool rows16 = ((long long)ny * (m + 1) * vs) % 16 == 0;  // cp.async tiles need 16-byte row starts
     for (int i = 0; i < nb && !P.fb; ++i)
-        if (vb[i].nx == nx && seen++ == idx_b) P.fb = &vb[i];
+        if (vb[i].nx == nx && (vb[i].kind == 0 || rows16) && seen++ == idx_b) P.fb = &vb[i];
     if (P.fa) {
         for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.fa->smem);
@@ -177,10 +237,19 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, P.fa->kfwd, P.fa->nt, P.fa->smem);
         P.occ_fa = std::max(occ, 1);
         const size_t plane = (size_t)ny * (m + 1) * vs;
-        const int K = choose_cluster(P.device, nx, ny, m, P.fa->wy, plane, P.occ_fa, sms);
+        int K = choose_cluster(P.device, nx, ny, m, P.fa->wy, plane, P.occ_fa, sms);
+        if (P.fa->kind == 1) {
+            // the plane lives in the cluster's shared memory: the cluster size is fixed
+            K = P.fa->k;
+            if (K > 8) {
+                cudaFuncSetAttribute(P.fa->kfwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                cudaFuncSetAttribute(P.fa->kinv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            }
+        }
         const int mc = max_clusters(P.fa->kfwd, K, nx, P.fa->smem, P.fa->nt, std::max(1, P.occ_fa * sms / K));
         P.k_fa = K;
         P.grid_fa = K * std::min(nx, mc);
+        if (P.fa->kind == 1 && mc < 1) P.fa = nullptr;
     }
     if (P.fb) {
         for (const void *k : {P.fb->kfwd, P.fb->kinv}) {
@@ -200,6 +269,169 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         const long long tiles = (ncols + P.fb->w - 1) / P.fb->w;
         P.grid_fb = (int)std::min<long long>(tiles, (long long)P.occ_fb * sms);
     }
+    return P.dtype == GPUFFT_FLOAT ? upload_stage_tables<float>(P) : upload_stage_tables<double>(P);
+}
+
+// ---------------------------------------------------------------------------
+// wisdom: (device, dtype, grid) -> chosen candidate per pass
+// ---------------------------------------------------------------------------
+namespace {
+using WisdomKey = std::tuple<std::string, int, long long, long long, long long>;
+std::mutex g_wisdom_mu;
+std::map<WisdomKey, std::pair<int, int>> g_wisdom;
+bool g_wisdom_env_loaded = false;
+}  // namespace
+
+static std::string device_tag(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+    std::string name = prop.name;
+    for (auto &c : name)
+        if (c == ' ') c = '_';
+    return name + "_sm" + std::to_string(prop.major * 10 + prop.minor);
+}
+
+static WisdomKey wisdom_key(const Plan &P) {
+    return WisdomKey(device_tag(P.device), P.dtype, (long long)P.nx, (long long)P.ny, (long long)P.nz);
+}
+
+static int wisdom_load_locked(const char *path) {
+    std::ifstream in(path);
+    if (!in) return set_error(GPUFFT_ERR_INVALID, "cannot read wisdom file %s", path);
+    std::string line;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::istringstream ss(line);
+        std::string dev;
+        int dt, a, b;
+        long long nx, ny, nz;
+        if (ss >> dev >> dt >> nx >> ny >> nz >> a >> b) g_wisdom[WisdomKey(dev, dt, nx, ny, nz)] = {a, b};
+    }
+    return GPUFFT_SUCCESS;
+}
+
+static int wisdom_save_locked(const char *path) {
+    std::ofstream out(path);
+    if (!out) return set_error(GPUFFT_ERR_INVALID, "cannot write wisdom file %s", path);
+    out << "# gpufft_b200 wisdom: device dtype nx ny nz passA_candidate passB_candidate\n";
+    for (const auto &kv : g_wisdom)
+        out << std::get<0>(kv.first) << " " << std::get<1>(kv.first) << " " << std::get<2>(kv.first) << " "
+            << std::get<3>(kv.first) << " " << std::get<4>(kv.first) << " " << kv.second.first << " "
+            << kv.second.second << "\n";
+    return GPUFFT_SUCCESS;
+}
+
+int wisdom_save(const char *path) {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    return wisdom_save_locked(path);
+}
+
+int wisdom_load(const char *path) {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    return wisdom_load_locked(path);
+}
+
+static bool wisdom_lookup(const Plan &P, int &ia, int &ib) {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    if (!g_wisdom_env_loaded) {
+        g_wisdom_env_loaded = true;
+        const char *path = std::getenv("GPUFFT_WISDOM");
+        if (path) {
+            std::ifstream probe(path);
+            if (probe) wisdom_load_locked(path);
+        }
+    }
+    auto it = g_wisdom.find(wisdom_key(P));
+    if (it == g_wisdom.end()) return false;
+    ia = it->second.first;
+    ib = it->second.second;
+    return true;
+}
+
+static void wisdom_store(const Plan &P) {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    g_wisdom[wisdom_key(P)] = {P.idx_a, P.idx_b};
+    const char *path = std::getenv("GPUFFT_WISDOM");
+    if (path) wisdom_save_locked(path);
+}
+
+static int count_candidates(const Plan &P, int pass) {
+    const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
+    int n = 0;
+    if (pass == 0) {
+        const fast::VariantA *va = P.dtype == GPUFFT_FLOAT ? fast::kVariantsA_f32 : fast::kVariantsA_f64;
+        const int na = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsA_f32 : fast::kNumVariantsA_f64;
+        for (int i = 0; i < na; ++i) n += (va[i].ny == ny && va[i].m == m);
+    } else {
+        const fast::VariantB *vb = P.dtype == GPUFFT_FLOAT ? fast::kVariantsB_f32 : fast::kVariantsB_f64;
+        const int nb = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsB_f32 : fast::kNumVariantsB_f64;
+        const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
+        for (int i = 0; i < nb; ++i) n += (vb[i].nx == nx && (vb[i].kind == 0 || rows16));
+    }
+    return n;
+}
+
+static int plan_exec_pass_impl(const Plan *P, void *data, void *stream, int pass, bool forward);
+
+// mean ms of forward + inverse of one pass over `reps` repetitions
+static float time_pass(const Plan &P, void *data, cudaStream_t s, int pass, int reps) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int w = 0; w < 2; ++w) {
+        plan_exec_pass_impl(&P, data, s, pass, true);
+        plan_exec_pass_impl(&P, data, s, pass, false);
+    }
+    cudaEventRecord(e0, s);
+    int rc = GPUFFT_SUCCESS;
+    for (int r = 0; r < reps && rc == GPUFFT_SUCCESS; ++r) {
+        rc = plan_exec_pass_impl(&P, data, s, pass, true);
+        if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass_impl(&P, data, s, pass, false);
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != GPUFFT_SUCCESS || cudaGetLastError() != cudaSuccess) return 1e30f;
+    return ms / reps;
+}
+
+int plan_autotune(Plan *P, void *scratch, void *stream) {
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = (size_t)P->nx * P->ny * (P->nz / 2 + 1) * (P->dtype == GPUFFT_FLOAT ? 8 : 16);
+    void *buf = scratch;
+    if (!buf) {
+        cudaError_t e = cudaMalloc(&buf, bytes);
+        if (e != cudaSuccess)
+            return set_error(GPUFFT_ERR_OOM, "autotune scratch (%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    cudaMemsetAsync(buf, 0, bytes, s);
+    const int reps = bytes > (256u << 20) ? 3 : 10;
+    int best[2] = {-1, -1};
+    for (int pass = 0; pass < 2; ++pass) {
+        const int n = count_candidates(*P, pass);
+        float best_ms = 1e30f;
+        for (int c = -1; c < n; ++c) {
+            if (pass == 0)
+                setup_fast(*P, c, P->idx_b);
+            else
+                setup_fast(*P, best[0], c);
+            if ((pass == 0 && c >= 0 && !P->fa) || (pass == 1 && c >= 0 && !P->fb)) continue;
+            const float ms = time_pass(*P, buf, s, pass, reps);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best[pass] = c;
+            }
+        }
+    }
+    if (!scratch) cudaFree(buf);
+    const int rc = setup_fast(*P, best[0], best[1]);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    P->tuned = true;
+    wisdom_store(*P);
     return GPUFFT_SUCCESS;
 }
 
@@ -306,11 +538,19 @@ static int build_plan(Plan &P) {
     P.grid_b = (int)std::min<long long>(B.ntiles, (long long)occ_b * sms);
     P.occ_a = occ_a;
     P.occ_b = occ_b;
-    if (!std::getenv("GPUFFT_GENERIC_ONLY")) setup_fast(P, 0, 0);
-    return GPUFFT_SUCCESS;
+    if (std::getenv("GPUFFT_GENERIC_ONLY")) {
+        P.idx_a = P.idx_b = -1;
+        return GPUFFT_SUCCESS;
+    }
+    int ia = 0, ib = 0;
+    if (wisdom_lookup(P, ia, ib)) P.tuned = true;
+    const char *va = std::getenv("GPUFFT_VARIANT_A"), *vb = std::getenv("GPUFFT_VARIANT_B");
+    if (va) ia = std::atoi(va);
+    if (vb) ib = std::atoi(vb);
+    return setup_fast(P, ia, ib);
 }
 
-int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype) {
+int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags) {
     if (!out) return set_error(GPUFFT_ERR_INVALID, "plan pointer is NULL");
     *out = nullptr;
     if (nx < 1 || ny < 1 || nz < 1)
@@ -329,6 +569,11 @@ int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype) {
     if (e != cudaSuccess) { delete P; return cuda_error(e, "cudaGetDevice"); }
     const int rc = dtype == GPUFFT_FLOAT ? build_plan<float>(*P) : build_plan<double>(*P);
     if (rc != GPUFFT_SUCCESS) { plan_destroy(P); return rc; }
+    const char *env = std::getenv("GPUFFT_AUTOTUNE");
+    if (((flags & GPUFFT_PLAN_AUTOTUNE) || (env && env[0] == '1')) && !P->tuned) {
+        const int rt = plan_autotune(P, nullptr, nullptr);
+        if (rt != GPUFFT_SUCCESS) { plan_destroy(P); return rt; }
+    }
     *out = P;
     return GPUFFT_SUCCESS;
 }
@@ -340,6 +585,7 @@ int plan_destroy(Plan *P) {
         cudaGetDevice(&cur);
         if (cur != P->device) cudaSetDevice(P->device);
         cudaFree(P->tw_dev);
+        if (P->stage_dev) cudaFree(P->stage_dev);
         if (cur != P->device && cur >= 0) cudaSetDevice(cur);
     }
     delete P;
@@ -390,7 +636,7 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd) {
     if (P.nx == 1) return GPUFFT_SUCCESS;  // a length-1 DFT is the identity
     PassBParams prm = P.pb;
     prm.data = data;
-    if (P.fb) {
+    if (P.fb && !(P.fb->kind == 1 && ((uintptr_t)data) % 16 != 0)) {
         prm.wx = P.fb->w;
         prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
         void *args[] = {&prm};
@@ -434,6 +680,10 @@ int plan_exec(const Plan *P, void *data, void *stream, bool forward) {
 }
 
 int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward) {
+    return plan_exec_pass_impl(P, data, stream, pass, forward);
+}
+
+static int plan_exec_pass_impl(const Plan *P, void *data, void *stream, int pass, bool forward) {
     if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
     if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
     if (((uintptr_t)data) % (P->dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
@@ -462,8 +712,9 @@ int plan_describe(const Plan *P, char *buf, int len) {
     if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
     std::string s;
     char b[256];
-    snprintf(b, sizeof(b), "grid=%lldx%lldx%lld dtype=%s ", (long long)P->nx, (long long)P->ny, (long long)P->nz,
-             P->dtype == GPUFFT_FLOAT ? "f32" : "f64");
+    snprintf(b, sizeof(b), "grid=%lldx%lldx%lld dtype=%s tuned=%d candA=%d candB=%d ", (long long)P->nx,
+             (long long)P->ny, (long long)P->nz, P->dtype == GPUFFT_FLOAT ? "f32" : "f64", P->tuned ? 1 : 0, P->idx_a,
+             P->idx_b);
     s += b;
     describe_axis(s, "x", P->pb.ax);
     s += " ";
@@ -476,12 +727,12 @@ int plan_describe(const Plan *P, char *buf, int len) {
              P->pb.wx, P->pb.ntiles);
     s += b;
     if (P->fa) {
-        snprintf(b, sizeof(b), " fastA{ny=%d m=%d wz=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu}", P->fa->ny, P->fa->m,
-                 P->fa->wz, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa, P->fa->smem);
+        snprintf(b, sizeof(b), " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu}", P->fa->kind, P->fa->ny, P->fa->m,
+                 P->fa->rw, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa, P->fa->smem);
         s += b;
     }
     if (P->fb) {
-        snprintf(b, sizeof(b), " fastB{nx=%d w=%d nt=%d v=%d grid=%d occ=%d smem=%zu}", P->fb->nx, P->fb->w,
+        snprintf(b, sizeof(b), " fastB{kind=%d nx=%d w=%d nt=%d v=%d grid=%d occ=%d smem=%zu}", P->fb->kind, P->fb->nx, P->fb->w,
                  P->fb->nt, P->fb->v, P->grid_fb, P->occ_fb, P->fb->smem);
         s += b;
     }
@@ -509,7 +760,7 @@ extern "C" int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int pr
         return set_error(GPUFFT_ERR_UNSUPPORTED, "procs=%d rank=%d: only a size-1 communicator is supported", procs,
                          rank);
     Plan *P = nullptr;
-    const int rc = plan_create(&P, nx, ny, nz, dtype);
+    const int rc = plan_create(&P, nx, ny, nz, dtype, 0);
     if (rc != GPUFFT_SUCCESS) return rc;
     std::lock_guard<std::mutex> lk(g_mu);
     plan_destroy(g_global[dtype]);
@@ -551,10 +802,28 @@ extern "C" int gpufft_finalize(void) {
 extern "C" const char *gpufft_last_error(void) { return last_error(); }
 
 extern "C" int gpufft_plan_create(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype) {
+    return gpufft_plan_create_ex(plan, nx, ny, nz, dtype, 0);
+}
+
+extern "C" int gpufft_plan_create_ex(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags) {
     Plan *P = nullptr;
-    const int rc = plan_create(&P, nx, ny, nz, dtype);
+    const int rc = plan_create(&P, nx, ny, nz, dtype, flags);
     if (plan) *plan = reinterpret_cast<gpufft_plan>(P);
     return rc;
+}
+
+extern "C" int gpufft_plan_autotune(gpufft_plan plan, void *scratch, void *stream) {
+    return plan_autotune(reinterpret_cast<Plan *>(plan), scratch, stream);
+}
+
+extern "C" int gpufft_wisdom_save(const char *path) {
+    if (!path) return set_error(GPUFFT_ERR_INVALID, "wisdom path is NULL");
+    return wisdom_save(path);
+}
+
+extern "C" int gpufft_wisdom_load(const char *path) {
+    if (!path) return set_error(GPUFFT_ERR_INVALID, "wisdom path is NULL");
+    return wisdom_load(path);
 }
 
 extern "C" int gpufft_plan_destroy(gpufft_plan plan) { return plan_destroy(reinterpret_cast<Plan *>(plan)); }

@@ -13,7 +13,8 @@ struct Plan {
     int64_t nx = 0, ny = 0, nz = 0;
     int dtype = 0;
     int device = 0;
-    void *tw_dev = nullptr;  // x, y, z twiddle tables back to back
+    void *tw_dev = nullptr;     // x, y, z twiddle tables back to back
+    void *stage_dev = nullptr;  // per-stage tables of the specialised kernels
     PassAParams pa{};
     PassBParams pb{};
     size_t smem_a = 0, smem_b = 0;
@@ -23,15 +24,20 @@ struct Plan {
     const fast::VariantA *fa = nullptr;
     const fast::VariantB *fb = nullptr;
     int grid_fa = 0, grid_fb = 0, k_fa = 1, occ_fa = 0, occ_fb = 0;
+    int idx_a = 0, idx_b = 0;  // registry candidate in use per pass (-1 = generic kernels)
+    bool tuned = false;
 };
 
 int set_error(int code, const char *fmt, ...);
 const char *last_error();
-int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype);
+int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
 int plan_destroy(Plan *P);
 int plan_exec(const Plan *P, void *data, void *stream, bool forward);
 int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward);
 int plan_launches(const Plan *P);
 int plan_describe(const Plan *P, char *buf, int len);
+int plan_autotune(Plan *P, void *scratch, void *stream);
+int wisdom_save(const char *path);
+int wisdom_load(const char *path);
 
 }  // namespace gpufft

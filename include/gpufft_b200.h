@@ -91,6 +91,30 @@ int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream);
  * strided 1D C2C plan, GPU_FFT_init.cu:59-92.) */
 int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int forward);
 
+/* --------------------------------------------------------------------------
+ * Autotuning and wisdom.  The reference's INIT builds fixed cuFFT plans
+ * (GPU_FFT_init.cu:86-91); here a plan chooses among several compiled kernel
+ * shapes per pass (radix lists, tile widths, threads per CTA, cluster
+ * layouts).  Autotuning times every candidate on a field-sized buffer and
+ * keeps the fastest; the choice is remembered per device and grid
+ * ("wisdom"), and can be saved to / loaded from a text file.  If the
+ * environment variable GPUFFT_AUTOTUNE is set to 1, gpufft_init and
+ * gpufft_plan_create autotune; if GPUFFT_WISDOM names a file, plans read it
+ * and autotuning appends to it.
+ * ------------------------------------------------------------------------ */
+#define GPUFFT_PLAN_AUTOTUNE 1
+
+int gpufft_plan_create_ex(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
+
+/* Times the candidates of both passes on `scratch` (a device buffer of
+ * gpufft_field_bytes() bytes whose contents are overwritten; NULL = allocate a
+ * temporary one) on `stream`, keeps the fastest, records it in the wisdom.
+ * Synchronises the stream. */
+int gpufft_plan_autotune(gpufft_plan plan, void *scratch, void *stream);
+
+int gpufft_wisdom_save(const char *path);
+int gpufft_wisdom_load(const char *path);
+
 /* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
 int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);
 

@@ -80,6 +80,22 @@ def test_argument_errors_are_reported_without_a_gpu(lib):
     assert not h.value
     assert lib.gpufft_exec_r2c(None, ctypes.c_void_p(16), None) == 4
     assert lib.gpufft_plan_destroy(None) == 0
+    assert lib.gpufft_plan_autotune(None, None, None) == 4
+    assert lib.gpufft_wisdom_save(None) == 1
+    assert lib.gpufft_wisdom_load(b"/nonexistent/dir/wisdom.txt") == 1
+
+
+def test_wisdom_file_round_trip(lib, tmp_path):
+    """Wisdom files hold one line per (device, dtype, grid); loading and saving
+    them needs no GPU."""
+    src = tmp_path / "w1.txt"
+    src.write_text("# comment\nNVIDIA_B200_sm100 0 512 512 512 0 1\nNVIDIA_B200_sm100 1 128 128 128 -1 0\n")
+    assert lib.gpufft_wisdom_load(str(src).encode()) == 0
+    dst = tmp_path / "w2.txt"
+    assert lib.gpufft_wisdom_save(str(dst).encode()) == 0
+    lines = [l for l in dst.read_text().splitlines() if not l.startswith("#")]
+    assert "NVIDIA_B200_sm100 0 512 512 512 0 1" in lines
+    assert "NVIDIA_B200_sm100 1 128 128 128 -1 0" in lines
 
 
 def test_python_binding_errors(lib):

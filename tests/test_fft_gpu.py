@@ -321,3 +321,28 @@ def test_specialised_kernels_agree_with_generic(oracle, cuda, grid, monkeypatch)
     generic.c2r(b)
     torch.cuda.synchronize()
     assert ((a - b).double().norm() / b.double().norm()).item() < 1e-6
+
+
+def test_autotune_keeps_results_identical_and_records_wisdom(oracle, cuda, tmp_path):
+    """Autotuning picks among compiled candidates (and the generic kernels); the
+    transform stays within tolerance of the oracle, and the choice is saved to
+    and reloaded from a wisdom file."""
+    import torch
+    import gpu_fft_b200 as g
+
+    grid = (128, 128, 128)
+    p = g.Plan(*grid, "float", autotune=True)
+    assert "tuned=1" in p.describe()
+    f = oracle.uniform_field(*grid, seed=8, dtype=np.float32)
+    d = torch.from_numpy(f.copy()).cuda()
+    p.r2c(d)
+    torch.cuda.synchronize()
+    got = d.cpu().numpy().view(np.complex64).reshape(128, 128, 65)
+    assert oracle.rel_l2(got, oracle.c_r2c(f.astype(np.float64), *grid)) < TOL["float"]
+    path = str(tmp_path / "wisdom.txt")
+    g.wisdom_save(path)
+    text = open(path).read()
+    assert " 0 128 128 128 " in text
+    g.wisdom_load(path)
+    q = g.Plan(*grid, "float")
+    assert "tuned=1" in q.describe()
