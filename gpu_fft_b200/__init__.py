@@ -29,6 +29,7 @@ EXPORTS = (
     "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_exec_r2c", "gpufft_exec_c2r",
     "gpufft_exec_pass", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
     "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
+    "gpufft_exec_noalloc",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 

@@ -115,6 +115,19 @@ int gpufft_plan_autotune(gpufft_plan plan, void *scratch, void *stream);
 int gpufft_wisdom_save(const char *path);
 int gpufft_wisdom_load(const char *path);
 
+/* No counterpart in the reference.  In-place transform of `data` on
+ * `stream` (forward != 0: R2C, else C2R, same layout and results as
+ * gpufft_r2c / gpufft_c2r) that allocates no device memory, for callers that
+ * cannot call cudaMalloc: a device heap owned by an external allocator,
+ * allocation-free sections of a serving loop, pre-partitioned device memory.
+ * Its twiddle tables live in a static device array of 192 KiB that every GPU
+ * loading the library holds until exit; every axis must be at most 4096
+ * (larger grids are rejected with GPUFFT_ERR_UNSUPPORTED).  Every call
+ * rewrites that array, so calls that overlap on the GPU race: serialise
+ * them.  The first call on each device looks up the array's address; make
+ * that first call before any stream capture. */
+int gpufft_exec_noalloc(int64_t nx, int64_t ny, int64_t nz, int dtype, int forward, void *data, void *stream);
+
 /* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
 int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);
 
