@@ -29,6 +29,8 @@ const VariantA kVariantsA_f64[] = {
 const int kNumVariantsA_f64 = sizeof(kVariantsA_f64) / sizeof(kVariantsA_f64[0]);
 
 const VariantB kVariantsB_f64[] = {
+    P_ENTRY(double, 1, 512, 8, 256, 0, 2),
+    P_ENTRY(double, 1, 512, 4, 256, 0, 2),
     B_ENTRY(double, 1, 512, 8, 256, 0, 2),
     B_ENTRY(double, 1, 512, 4, 256, 0, 2),
     B_ENTRY(double, 1, 128, 8, 256, 0, 2),

@@ -346,3 +346,43 @@ def test_autotune_keeps_results_identical_and_records_wisdom(oracle, cuda, tmp_p
     g.wisdom_load(path)
     q = g.Plan(*grid, "float")
     assert "tuned=1" in q.describe()
+
+
+@pytest.mark.parametrize("grid,dt", [((512, 512, 512), "float"), ((512, 512, 512), "double"),
+                                     ((1024, 512, 256), "float"), ((256, 256, 256), "float")], ids=str)
+def test_every_compiled_candidate_matches_generic(cuda, grid, dt, monkeypatch):
+    """The autotuner picks on speed alone, so every registered kernel candidate
+    of both passes must compute the same transform as the generic kernels."""
+    import torch
+    import gpu_fft_b200 as g
+
+    tdt = _torch_dt(dt)
+    nx, ny, nz = grid
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    f = torch.zeros((nx, ny, 2 * (nz // 2 + 1)), dtype=tdt, device="cuda")
+    f[:, :, :nz] = torch.randn((nx, ny, nz), generator=gen, dtype=tdt, device="cuda")
+    monkeypatch.setenv("GPUFFT_GENERIC_ONLY", "1")
+    ref = g.Plan(nx, ny, nz, dt)
+    monkeypatch.delenv("GPUFFT_GENERIC_ONLY")
+    s = torch.cuda.current_stream().cuda_stream
+    want = {}
+    for which in (0, 1):
+        for fwd in (True, False):
+            x = f.clone()
+            ref.pass_ptr(x.data_ptr(), s, which, fwd)
+            want[(which, fwd)] = x
+    tol = 1e-6 if dt == "float" else 1e-13
+    for which, env, tag in ((0, "GPUFFT_VARIANT_A", "fastA"), (1, "GPUFFT_VARIANT_B", "fastB")):
+        for c in range(16):
+            monkeypatch.setenv(env, str(c))
+            p = g.Plan(nx, ny, nz, dt)
+            if tag not in p.describe():
+                break
+            for fwd in (True, False):
+                x = f.clone()
+                p.pass_ptr(x.data_ptr(), s, which, fwd)
+                torch.cuda.synchronize()
+                w = want[(which, fwd)]
+                err = ((x - w).double().norm() / w.double().norm()).item()
+                assert err < tol, (tag, c, fwd, err, p.describe())
+        monkeypatch.delenv(env)
