@@ -30,6 +30,8 @@ EXPORTS = (
     "gpufft_exec_pass", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
     "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
     "gpufft_exec_noalloc",
+    "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
+    "gpufft_batch_status", "gpufft_batch_items",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 
@@ -69,6 +71,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_plan_autotune.argtypes = [vp, vp, vp]
     lib.gpufft_wisdom_save.argtypes = [ctypes.c_char_p]
     lib.gpufft_wisdom_load.argtypes = [ctypes.c_char_p]
+    lib.gpufft_exec_noalloc.argtypes = [i64, i64, i64, ci, ci, vp, vp]
+    lib.gpufft_batch_create.argtypes = [ctypes.POINTER(vp), ci, ctypes.POINTER(i64), ctypes.POINTER(ci), ci]
+    lib.gpufft_batch_destroy.argtypes = [vp]
+    lib.gpufft_batch_exec.argtypes = [vp, ctypes.POINTER(vp), vp]
+    lib.gpufft_batch_exec_graph.argtypes = [vp, ctypes.POINTER(vp), vp]
+    lib.gpufft_batch_status.argtypes = [vp, vp]
+    lib.gpufft_batch_items.argtypes = [vp]
     for name in EXPORTS:
         if getattr(lib, name, None) is None:
             raise ImportError(f"{path} does not export {name}")
@@ -176,6 +185,62 @@ class Plan:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().gpufft_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent in-place transforms (mixed grids, each R2C or C2R) in one
+    persistent kernel launch (gpufft_batch_*).  grids: list of (Nx, Ny, Nz);
+    directions: list of "r2c"/"c2r" (or 1/0)."""
+
+    def __init__(self, grids, directions, dtype="float"):
+        lib = load_library()
+        self.grids = [tuple(int(v) for v in g) for g in grids]
+        self.n = len(self.grids)
+        dirs = [1 if d in (1, True, "r2c", "forward") else 0 for d in directions]
+        if len(dirs) != self.n:
+            raise ValueError("one direction per grid")
+        self.directions = dirs
+        self.dtype_code = _dtype_code(dtype)
+        dims = (ctypes.c_int64 * (3 * self.n))(*[v for g in self.grids for v in g])
+        dd = (ctypes.c_int * self.n)(*dirs)
+        h = ctypes.c_void_p()
+        _check(lib.gpufft_batch_create(ctypes.byref(h), self.n, dims, dd, self.dtype_code))
+        self._h = h
+
+    def _ptrs(self, fields):
+        if len(fields) != self.n:
+            raise ValueError(f"expected {self.n} fields")
+        for f, (nx, ny, nz) in zip(fields, self.grids):
+            need = nx * ny * nh_of(nz) * (8 if self.dtype_code == GPUFFT_FLOAT else 16)
+            if not f.is_cuda or not f.is_contiguous() or f.numel() * f.element_size() < need:
+                raise ValueError("each field must be a contiguous CUDA tensor of its grid's size")
+        return (ctypes.c_void_p * self.n)(*[f.data_ptr() for f in fields])
+
+    def exec(self, fields, stream=None, graph=False):
+        fn = load_library().gpufft_batch_exec_graph if graph else load_library().gpufft_batch_exec
+        _check(fn(self._h, self._ptrs(fields), _stream_handle(stream)))
+        return fields
+
+    def exec_ptrs(self, ptrs, stream: int = 0, graph=False):
+        fn = load_library().gpufft_batch_exec_graph if graph else load_library().gpufft_batch_exec
+        _check(fn(self._h, (ctypes.c_void_p * self.n)(*ptrs), stream))
+
+    def status(self, stream=None) -> None:
+        _check(load_library().gpufft_batch_status(self._h, _stream_handle(stream)))
+
+    def items(self) -> int:
+        return int(load_library().gpufft_batch_items(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

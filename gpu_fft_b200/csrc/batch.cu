@@ -1,0 +1,372 @@
+// batch.cu — many independent transforms of mixed grids and directions in one
+// persistent kernel launch (replayable as a CUDA graph).
+//
+// The reference transforms one grid per call (GPU_FFT_R2C / GPU_FFT_C2R,
+// FFT_R2C.cu:41-70); a spectral solver calls it for several fields per step.
+// Here a batch of transforms is one launch of a persistent kernel fed by a
+// work queue in global memory:
+//   items = [first-pass items of every transform] ++ [second-pass items]
+// where for a forward transform the first pass is Pass A (one x-plane per
+// item: z R2C rows, block barrier, y columns) and the second is Pass B (one
+// tile of x-pencils per item); for an inverse the order is reversed.  A CTA
+// takes the next item with an atomic counter.  A second-pass item of
+// transform t waits until the first-pass items of t are complete (a counter
+// per transform, release/acquire at GPU scope).  All first-pass items are
+// taken before any second-pass item and nothing waits inside the first
+// pass, so every wait ends; the wait is still bounded (about two seconds),
+// after which the kernel records an error and skips the item.
+//
+// The items run the size-generic device code of fft_kernels.cuh with each
+// transform's own radix plan and twiddle tables, so one kernel serves any mix
+// of grids.  Scratch: the queue head, one counter per transform and an error
+// word, cleared by a memset node before every launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/gpufft_b200.h"
+#include "fft_kernels.cuh"
+#include "gpufft_internal.h"
+
+namespace gpufft {
+
+struct BatchDesc {
+    PassAParams pa;  // generic Pass A parameters (cluster size 1)
+    PassBParams pb;  // generic Pass B parameters
+    int forward;
+    int n_first;     // number of first-pass items
+    int smem_elems;  // complex elements of shared memory any item of it needs
+};
+
+struct BatchItem {
+    int t;      // transform
+    int pass;   // 0 = Pass A (plane index), 1 = Pass B (tile index)
+    int index;
+    int second; // 1 when it depends on the first pass of t
+};
+
+struct BatchScratch {
+    int head;
+    int err;
+    int done[1];  // one per transform (allocated longer)
+};
+
+constexpr long long kBatchWaitSpins = 1LL << 22;  // x ~500 ns sleep: about 2 s
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <typename T>
+__device__ void batch_plane(const BatchDesc &D, int x, unsigned char *smem) {
+    using V = cx_t<T>;
+    const PassAParams &P = D.pa;
+    V *twz = reinterpret_cast<V *>(smem);
+    V *twy = twz + P.nz;
+    V *ta = twy + P.ny;
+    V *tb = ta + P.tile_elems;
+    for (int q = threadIdx.x; q < P.nz; q += kThreads) twz[q] = reinterpret_cast<const V *>(P.twz)[q];
+    for (int q = threadIdx.x; q < P.ny; q += kThreads) twy[q] = reinterpret_cast<const V *>(P.twy)[q];
+    __syncthreads();
+    V *g = reinterpret_cast<V *>(P.data) + (long long)x * P.ny * P.nh;
+    const int ntiles_y = (P.m + P.wy - 1) / P.wy;
+    if (D.forward) {
+        for (int r0 = 0; r0 < P.ny; r0 += P.wz) rows_r2c<T>(P, g, ta, tb, twz, r0, min(P.wz, P.ny - r0));
+        __syncthreads();
+        for (int t = 0; t < ntiles_y; ++t) cols_y<T, true>(P, g, ta, tb, twy, t * P.wy, min(P.wy, P.m - t * P.wy));
+    } else {
+        for (int t = 0; t < ntiles_y; ++t) cols_y<T, false>(P, g, ta, tb, twy, t * P.wy, min(P.wy, P.m - t * P.wy));
+        __syncthreads();
+        for (int r0 = 0; r0 < P.ny; r0 += P.wz) rows_c2r<T>(P, g, ta, tb, twz, r0, min(P.wz, P.ny - r0));
+    }
+}
+
+template <typename T>
+__device__ void batch_tile(const BatchDesc &D, long long tile, unsigned char *smem) {
+    using V = cx_t<T>;
+    const PassBParams &P = D.pb;
+    V *twx = reinterpret_cast<V *>(smem);
+    V *ta = twx + P.nx;
+    V *tb = ta + (size_t)P.nx * P.wx;
+    for (int q = threadIdx.x; q < P.nx; q += kThreads) twx[q] = reinterpret_cast<const V *>(P.twx)[q];
+    __syncthreads();
+    V *base = reinterpret_cast<V *>(P.data);
+    const long long c0 = tile * P.wx;
+    const int wv = (int)min((long long)P.wx, P.ncols - c0);
+    load_cols<T>(ta, base + c0, P.ncols, P.nx, P.wx, P.wxdiv, wv);
+    __syncthreads();
+    V *res = D.forward ? fft_tile<T, true>(ta, tb, P.wx, 1, P.wx, P.wxdiv, P.ax, twx)
+                       : fft_tile<T, false>(ta, tb, P.wx, 1, P.wx, P.wxdiv, P.ax, twx);
+    store_cols<T>(res, base + c0, P.ncols, P.nx, P.wx, P.wxdiv, 0, wv);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) batch_kernel(const BatchDesc *__restrict__ descs,
+                                                         const BatchItem *__restrict__ items, int nitems,
+                                                         BatchScratch *scratch) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item;
+    __shared__ int s_skip;
+    for (;;) {
+        __syncthreads();  // previous item's shared-memory use is over
+        if (threadIdx.x == 0) s_item = atomicAdd(&scratch->head, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) return;
+        const BatchItem item = items[it];
+        const BatchDesc &D = descs[item.t];
+        if (item.second) {
+            if (threadIdx.x == 0) {
+                int skip = 1;
+                for (long long spin = 0; spin < kBatchWaitSpins; ++spin) {
+                    if (ld_acquire(&scratch->done[item.t]) >= D.n_first) {
+                        skip = 0;
+                        break;
+                    }
+                    __nanosleep(500);
+                }
+                if (skip) atomicExch(&scratch->err, 1);
+                s_skip = skip;
+            }
+            __syncthreads();
+            if (s_skip) continue;
+        }
+        if (item.pass == 0)
+            batch_plane<T>(D, item.index, smem_raw);
+        else
+            batch_tile<T>(D, item.index, smem_raw);
+        if (!item.second) {
+            __syncthreads();  // every thread's writes of this item are issued
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(&scratch->done[item.t], 1);
+            }
+        }
+    }
+}
+
+struct Batch {
+    int n = 0;
+    int dtype = 0;
+    int device = 0;
+    std::vector<Plan *> plans;
+    std::vector<int> forward;
+    std::vector<BatchDesc> hdesc;
+    std::vector<BatchItem> hitems;
+    BatchDesc *ddesc = nullptr;
+    BatchItem *ditems = nullptr;
+    BatchScratch *dscratch = nullptr;
+    size_t scratch_bytes = 0;
+    size_t smem = 0;
+    int grid = 0;
+    // captured launch (scratch memset + kernel); replayed by gpufft_batch_exec_graph
+    cudaGraphExec_t gexec = nullptr;
+    bool gready = false;
+    std::vector<void *> uploaded;  // data pointers the device descriptors hold
+};
+
+static void batch_free(Batch *B) {
+    if (!B) return;
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    if (B->ddesc) cudaFree(B->ddesc);
+    if (B->ditems) cudaFree(B->ditems);
+    if (B->dscratch) cudaFree(B->dscratch);
+    for (Plan *p : B->plans) plan_destroy(p);
+    delete B;
+}
+
+template <typename T>
+static int batch_configure(Batch &B) {
+    using V = cx_t<T>;
+    size_t smem_elems = 0;
+    for (int t = 0; t < B.n; ++t) {
+        const Plan &P = *B.plans[t];
+        BatchDesc d;
+        std::memset(&d, 0, sizeof(d));
+        d.pa = P.pa;
+        d.pa.K = 1;
+        d.pb = P.pb;
+        d.forward = B.forward[t];
+        const int planes = (int)P.nx;
+        const long long tiles = P.nx == 1 ? 0 : P.pb.ntiles;
+        d.n_first = d.forward ? planes : (int)tiles;
+        const size_t ea = (size_t)P.pa.nz + P.pa.ny + 2 * (size_t)P.pa.tile_elems;
+        const size_t eb = (size_t)P.pb.nx + 2 * (size_t)P.pb.nx * P.pb.wx;
+        d.smem_elems = (int)std::max(ea, eb);
+        smem_elems = std::max(smem_elems, (size_t)d.smem_elems);
+        B.hdesc.push_back(d);
+    }
+    // first-pass items of every transform, then the second-pass items
+    for (int round = 0; round < 2; ++round)
+        for (int t = 0; t < B.n; ++t) {
+            const Plan &P = *B.plans[t];
+            const bool fwd = B.forward[t] != 0;
+            const int pass = (round == 0) == fwd ? 0 : 1;  // fwd: A first; inv: B first
+            if (pass == 0) {
+                for (int x = 0; x < (int)P.nx; ++x) B.hitems.push_back({t, 0, x, round});
+            } else if (P.nx > 1) {
+                for (long long j = 0; j < P.pb.ntiles; ++j) B.hitems.push_back({t, 1, (int)j, round});
+            }
+            if (round == 0 && pass == 1 && P.nx == 1) B.hdesc[t].n_first = 0;  // nothing to wait for
+        }
+    B.smem = smem_elems * sizeof(V);
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem);
+    if (e != cudaSuccess)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "batch needs %zu bytes of shared memory: %s", B.smem,
+                         cudaGetErrorString(e));
+    int occ = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<T>, kThreads, B.smem);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device);
+    B.grid = std::max(1, occ) * std::max(1, sms);
+    B.grid = (int)std::min<size_t>((size_t)B.grid, B.hitems.size() ? B.hitems.size() : 1);
+    return GPUFFT_SUCCESS;
+}
+
+static int batch_create(Batch **out, int n, const int64_t *dims, const int *directions, int dtype) {
+    if (!out) return set_error(GPUFFT_ERR_INVALID, "batch pointer is NULL");
+    *out = nullptr;
+    if (n < 1 || !dims || !directions) return set_error(GPUFFT_ERR_INVALID, "batch needs n >= 1, dims and directions");
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE)
+        return set_error(GPUFFT_ERR_INVALID, "dtype %d is neither GPUFFT_FLOAT nor GPUFFT_DOUBLE", dtype);
+    Batch *B = new (std::nothrow) Batch();
+    if (!B) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
+    B->n = n;
+    B->dtype = dtype;
+    cudaGetDevice(&B->device);
+    for (int t = 0; t < n; ++t) {
+        Plan *P = nullptr;
+        const int rc = plan_create(&P, dims[3 * t], dims[3 * t + 1], dims[3 * t + 2], dtype, 0);
+        if (rc != GPUFFT_SUCCESS) {
+            batch_free(B);
+            return rc;
+        }
+        B->plans.push_back(P);
+        B->forward.push_back(directions[t] != 0);
+    }
+    int rc = dtype == GPUFFT_FLOAT ? batch_configure<float>(*B) : batch_configure<double>(*B);
+    if (rc != GPUFFT_SUCCESS) {
+        batch_free(B);
+        return rc;
+    }
+    B->scratch_bytes = sizeof(BatchScratch) + sizeof(int) * (size_t)n;
+    cudaError_t e = cudaMalloc(&B->ddesc, sizeof(BatchDesc) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&B->ditems, sizeof(BatchItem) * std::max<size_t>(1, B->hitems.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&B->dscratch, B->scratch_bytes);
+    if (e != cudaSuccess) {
+        batch_free(B);
+        return set_error(GPUFFT_ERR_OOM, "batch tables: %s", cudaGetErrorString(e));
+    }
+    e = cudaMemcpy(B->ditems, B->hitems.data(), sizeof(BatchItem) * B->hitems.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        batch_free(B);
+        return set_error(GPUFFT_ERR_CUDA, "batch items: %s", cudaGetErrorString(e));
+    }
+    *out = B;
+    return GPUFFT_SUCCESS;
+}
+
+// the descriptors carry the data pointers; re-sent only when they change
+static int batch_upload(Batch &B, void *const *data, cudaStream_t s) {
+    if (B.uploaded.size() == (size_t)B.n && std::equal(B.uploaded.begin(), B.uploaded.end(), data))
+        return GPUFFT_SUCCESS;
+    for (int t = 0; t < B.n; ++t) {
+        if (!data[t]) return set_error(GPUFFT_ERR_INVALID, "batch data pointer %d is NULL", t);
+        if (((uintptr_t)data[t]) % (B.dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
+            return set_error(GPUFFT_ERR_INVALID, "batch data pointer %d is not aligned", t);
+        B.hdesc[t].pa.data = data[t];
+        B.hdesc[t].pb.data = data[t];
+    }
+    const cudaError_t e =
+        cudaMemcpyAsync(B.ddesc, B.hdesc.data(), sizeof(BatchDesc) * (size_t)B.n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "batch descriptors: %s", cudaGetErrorString(e));
+    B.uploaded.assign(data, data + B.n);
+    return GPUFFT_SUCCESS;
+}
+
+// clear the scratch, launch (the part a CUDA graph replays)
+static int batch_launch(Batch &B, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(B.dscratch, 0, B.scratch_bytes, s);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "batch scratch clear: %s", cudaGetErrorString(e));
+    const int nitems = (int)B.hitems.size();
+    if (B.dtype == GPUFFT_FLOAT)
+        batch_kernel<float><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch);
+    else
+        batch_kernel<double><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "batch launch: %s", cudaGetErrorString(e));
+}
+
+}  // namespace gpufft
+
+using namespace gpufft;
+
+extern "C" int gpufft_batch_create(gpufft_batch *batch, int n, const int64_t *dims, const int *directions, int dtype) {
+    Batch *B = nullptr;
+    const int rc = batch_create(&B, n, dims, directions, dtype);
+    if (batch) *batch = reinterpret_cast<gpufft_batch>(B);
+    return rc;
+}
+
+extern "C" int gpufft_batch_destroy(gpufft_batch batch) {
+    batch_free(reinterpret_cast<Batch *>(batch));
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_batch_exec(gpufft_batch batch, void *const *data, void *stream) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    if (!data) return set_error(GPUFFT_ERR_INVALID, "data array is NULL");
+    const int rc = batch_upload(*B, data, (cudaStream_t)stream);
+    return rc != GPUFFT_SUCCESS ? rc : batch_launch(*B, (cudaStream_t)stream);
+}
+
+extern "C" int gpufft_batch_exec_graph(gpufft_batch batch, void *const *data, void *stream) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    if (!data) return set_error(GPUFFT_ERR_INVALID, "data array is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = batch_upload(*B, data, s);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    if (!B->gready) {
+        // capture once: the scratch memset and the persistent kernel; the
+        // descriptors it reads are refreshed on the stream by batch_upload
+        cudaStream_t cs;
+        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "capture stream: %s", cudaGetErrorString(e));
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) rc = batch_launch(*B, cs);
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess || e2 != cudaSuccess || rc != GPUFFT_SUCCESS) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc != GPUFFT_SUCCESS ? rc : set_error(GPUFFT_ERR_CUDA, "batch capture failed");
+        }
+        e = cudaGraphInstantiate(&B->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        B->gready = true;
+    }
+    const cudaError_t e = cudaGraphLaunch(B->gexec, s);
+    return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+}
+
+extern "C" int gpufft_batch_status(gpufft_batch batch, void *stream) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, &B->dscratch->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "batch status: %s", cudaGetErrorString(e));
+    return err ? set_error(GPUFFT_ERR_CUDA, "batch: a dependent item gave up waiting") : GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_batch_items(gpufft_batch batch) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    return B ? (int)B->hitems.size() : 0;
+}

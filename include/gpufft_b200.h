@@ -128,6 +128,28 @@ int gpufft_wisdom_load(const char *path);
  * that first call before any stream capture. */
 int gpufft_exec_noalloc(int64_t nx, int64_t ny, int64_t nz, int dtype, int forward, void *data, void *stream);
 
+/* --------------------------------------------------------------------------
+ * Batches: many independent transforms (any mix of grids, each forward or
+ * inverse) in ONE persistent kernel launch fed by a work queue; a spectral
+ * solver's per-step set of fields (e.g. 3 velocity C2R + 6 product R2C) is
+ * one call.  The reference transforms one grid per call (GPU_FFT_R2C /
+ * GPU_FFT_C2R, FFT_R2C.cu:41-70, FFT_C2R.cu:41-70).  `dims` holds n triples
+ * (Nx, Ny, Nz); directions[t] is 1 for R2C, 0 for C2R; data[t] are the n
+ * in-place fields.  exec_graph captures the launch once into a CUDA graph and
+ * replays it (the data pointers may change between calls).  Scratch (queue
+ * head, one counter per transform) is owned by the batch.
+ * ------------------------------------------------------------------------ */
+typedef struct gpufft_batch_s *gpufft_batch;
+int gpufft_batch_create(gpufft_batch *batch, int n, const int64_t *dims, const int *directions, int dtype);
+int gpufft_batch_destroy(gpufft_batch batch);
+int gpufft_batch_exec(gpufft_batch batch, void *const *data, void *stream);
+int gpufft_batch_exec_graph(gpufft_batch batch, void *const *data, void *stream);
+/* Synchronises `stream`; GPUFFT_ERR_CUDA if an item of the last run gave up
+ * waiting for its dependency (bounded wait, about 2 s). */
+int gpufft_batch_status(gpufft_batch batch, void *stream);
+/* Work items per launch. */
+int gpufft_batch_items(gpufft_batch batch);
+
 /* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
 int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);
 
