@@ -522,6 +522,141 @@ def run_batch(args, world, rank):
     }
 
 
+# ---------------------------------------------------------------------------
+# precision form: FP32 vs BF16 / FP16 storage at 1024^3 on a turbulence field
+# ---------------------------------------------------------------------------
+def turbulence_on_gpu(n, seed=2025):
+    """k^-5/3 isotropic random-phase field on 1 <= |k| <= n/3, zero above, made
+    real by this library's FP64 C2R and scaled to unit RMS; float64 padded field."""
+    import math
+
+    import torch
+    import gpu_fft_b200 as g
+
+    nh = n // 2 + 1
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    k = torch.arange(n, device="cuda", dtype=torch.float64)
+    k = torch.where(k <= n // 2, k, k - n)
+    kz = torch.arange(nh, device="cuda", dtype=torch.float64)
+    buf = torch.empty((n, n, nh, 2), dtype=torch.float64, device="cuda")
+    for x in range(0, n, 64):  # build in slabs to bound temporaries
+        kk = torch.sqrt(k[x:x + 64, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2)
+        amp = torch.where((kk >= 1) & (kk <= n / 3.0), torch.sqrt(kk.clamp(min=1) ** (-5.0 / 3.0) / (4 * math.pi * kk.clamp(min=1) ** 2)),
+                          torch.zeros_like(kk))
+        ph = torch.rand(kk.shape, generator=gen, device="cuda", dtype=torch.float64) * (2 * math.pi)
+        buf[x:x + 64, :, :, 0] = amp * torch.cos(ph)
+        buf[x:x + 64, :, :, 1] = amp * torch.sin(ph)
+        del kk, amp, ph
+    field = buf.view(n, n, 2 * nh)
+    p64 = g.Plan(n, n, n, "double")
+    p64.c2r(field)
+    rms = torch.sqrt((field[:, :, :n] ** 2).mean())
+    field /= rms
+    field[:, :, n:] = 0
+    return field, p64
+
+
+def run_precision(args, world, rank):
+    import torch
+    import gpu_fft_b200 as g
+
+    n = args.nx if args.nx != NX else 1024
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    f64, p64 = turbulence_on_gpu(n)
+    ref = f64.clone()
+    p64.r2c(ref)
+    refc = ref.view(n, n, n // 2 + 1, 2)
+    ref_norm = refc.double().norm().item()
+    ref_max = refc.abs().max().item()
+    del p64
+
+    def errors(spec_fp32):
+        d = spec_fp32.view(n, n, n // 2 + 1, 2).double() - refc
+        return d.norm().item() / ref_norm, d.abs().max().item() / ref_max
+
+    out = {}
+    S32 = field_bytes(n, n, n, "float")
+    # ---- FP32 storage + compute
+    p32 = g.Plan(n, n, n, "float", autotune=not args.no_autotune)
+    x32 = f64.float()
+    y32 = x32.clone()
+    p32.r2c(y32)
+    e_l2, e_max = errors(y32)
+    del y32
+    ptr = x32.data_ptr()
+
+    def step32():
+        p32.r2c_ptr(ptr, sh)
+        p32.c2r_ptr(ptr, sh)
+
+    total, done = 0.0, 0
+    for _ in range(args.warmup):
+        x32.mul_(1.0 / n ** 3)
+        step32()
+    while done < args.steps:
+        k = min(4, args.steps - done)
+        x32.mul_(1.0 / n ** 3)
+        t, _ = time_steps(step32, k, 0, world, stream)
+        total += t
+        done += k
+    ms32 = total / args.steps
+    out["fp32"] = {"ms": round(ms32, 4), "rel_l2_vs_fp64": e_l2, "max_err_rel_to_max": e_max,
+                   "field_bytes": S32}
+    del x32
+    # ---- 16-bit storage, per-pencil scales, FP32 butterflies
+    for fmt in ("bf16", "fp16"):
+        p16 = g.Plan16(n, n, n, fmt)
+        field, scales = p16.empty()
+        src = f64.float()
+        p16.quantize(src, field, scales)
+        del src
+        work = field.clone()
+        wsc = scales.clone()
+        p16.r2c(work, wsc)
+        spec = torch.empty((n, n, n // 2 + 1, 2), dtype=torch.float32, device="cuda")
+        p16.dequantize(work, wsc, spec, spectrum=True)
+        e_l2, e_max = errors(spec)
+        del spec, work, wsc
+        fp, sp = field.data_ptr(), scales.data_ptr()
+
+        def step16():
+            p16.r2c_ptr(fp, sp, sh)
+            p16.c2r_ptr(fp, sp, sh)
+
+        total, done = 0.0, 0
+        for _ in range(args.warmup):
+            scales.mul_(1.0 / n ** 3)
+            step16()
+        while done < args.steps:
+            k = min(4, args.steps - done)
+            scales.mul_(1.0 / n ** 3)
+            t, _ = time_steps(step16, k, 0, world, stream)
+            total += t
+            done += k
+        ms16 = total / args.steps
+        out[fmt] = {"ms": round(ms16, 4), "rel_l2_vs_fp64": e_l2, "max_err_rel_to_max": e_max,
+                    "field_bytes": S32 // 2, "speedup_vs_fp32": round(ms32 / ms16, 3)}
+        del p16, field, scales
+    out["tc_split_bf16"] = {"status": "not built: the radix-16 stages run on the FP32 pipes"}
+    if rank != 0:
+        return None
+    peak, _ = load_peaks()
+    return {
+        "metric": f"precision form {n}^3: ms per R2C+C2R, BF16/FP16 storage vs FP32, error vs FP64",
+        "value": out["bf16"]["ms"], "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["bf16"]["ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 storage, f32 compute",
+        "data": "synthetic: k^-5/3 random-phase turbulence field (1 <= |k| <= N/3), unit RMS, built on the GPU",
+        "config": {"workload": f"precision form, {n}^3", "grid": [n, n, n],
+                   "reference": "this library's FP64 R2C of the same field"},
+        "variants": out,
+        "hbm_gbs_8S_fp32": round(8 * S32 / (out["fp32"]["ms"] * 1e-3) / 1e9, 1),
+        "hbm_gbs_8S_bf16": round(8 * (S32 // 2) / (out["bf16"]["ms"] * 1e-3) / 1e9, 1),
+        "peak_gbs": peak,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -534,7 +669,7 @@ def main():
     ap.add_argument("--dtype", choices=["float", "double"], default=DTYPE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the default kernel candidates")
-    ap.add_argument("--workload", choices=["headline", "batch64", "spectral"], default="headline",
+    ap.add_argument("--workload", choices=["headline", "batch64", "spectral", "precision"], default="headline",
                     help="headline: 512^3 R2C+C2R (the bench contract); batch64 / spectral: batched form")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -543,6 +678,8 @@ def main():
     try:
         if args.workload in ("batch64", "spectral"):
             res = run_batch(args, world, rank)
+        elif args.workload == "precision":
+            res = run_precision(args, world, rank)
         elif args.impl == "reference":
             res = run_reference(args, world, rank)
         else:

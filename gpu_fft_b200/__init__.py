@@ -32,6 +32,8 @@ EXPORTS = (
     "gpufft_exec_noalloc",
     "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
     "gpufft_batch_status", "gpufft_batch_items",
+    "gpufft_plan16_create", "gpufft_plan16_destroy", "gpufft_plan16_scale_count", "gpufft_exec16_r2c",
+    "gpufft_exec16_c2r", "gpufft_quantize16", "gpufft_dequantize16",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 
@@ -78,6 +80,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_batch_exec_graph.argtypes = [vp, ctypes.POINTER(vp), vp]
     lib.gpufft_batch_status.argtypes = [vp, vp]
     lib.gpufft_batch_items.argtypes = [vp]
+    lib.gpufft_plan16_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci]
+    lib.gpufft_plan16_destroy.argtypes = [vp]
+    lib.gpufft_plan16_scale_count.argtypes = [vp]
+    lib.gpufft_plan16_scale_count.restype = i64
+    lib.gpufft_exec16_r2c.argtypes = [vp, vp, vp, vp]
+    lib.gpufft_exec16_c2r.argtypes = [vp, vp, vp, vp]
+    lib.gpufft_quantize16.argtypes = [vp, vp, vp, vp, vp]
+    lib.gpufft_dequantize16.argtypes = [vp, vp, vp, vp, ci, vp]
     for name in EXPORTS:
         if getattr(lib, name, None) is None:
             raise ImportError(f"{path} does not export {name}")
@@ -241,6 +251,62 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().gpufft_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan16:
+    """Precision form: the field stored in BF16 ("bf16") or FP16 ("fp16") with one
+    FP32 scale per pencil, butterflies in FP32 (gpufft_plan16_*).  Fields are
+    uint16 tensors of 2*Nx*Ny*(Nz//2+1) elements; scales float32 tensors of
+    scale_count() elements."""
+
+    def __init__(self, nx: int, ny: int, nz: int, fmt="bf16"):
+        lib = load_library()
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.fmt = {"bf16": 0, "fp16": 1, 0: 0, 1: 1}[fmt]
+        h = ctypes.c_void_p()
+        _check(lib.gpufft_plan16_create(ctypes.byref(h), self.nx, self.ny, self.nz, self.fmt))
+        self._h = h
+
+    def scale_count(self) -> int:
+        return int(load_library().gpufft_plan16_scale_count(self._h))
+
+    def empty(self):
+        """(field, scales) device tensors for this grid."""
+        import torch
+
+        field = torch.empty(2 * self.nx * self.ny * nh_of(self.nz), dtype=torch.int16, device="cuda")
+        return field, torch.empty(self.scale_count(), dtype=torch.float32, device="cuda")
+
+    def quantize(self, real_fp32, field, scales, stream=None):
+        _check(load_library().gpufft_quantize16(self._h, real_fp32.data_ptr(), field.data_ptr(), scales.data_ptr(),
+                                                _stream_handle(stream)))
+
+    def dequantize(self, field, scales, out_fp32, spectrum: bool, stream=None):
+        _check(load_library().gpufft_dequantize16(self._h, field.data_ptr(), scales.data_ptr(), out_fp32.data_ptr(),
+                                                  1 if spectrum else 0, _stream_handle(stream)))
+
+    def r2c(self, field, scales, stream=None):
+        _check(load_library().gpufft_exec16_r2c(self._h, field.data_ptr(), scales.data_ptr(), _stream_handle(stream)))
+
+    def c2r(self, field, scales, stream=None):
+        _check(load_library().gpufft_exec16_c2r(self._h, field.data_ptr(), scales.data_ptr(), _stream_handle(stream)))
+
+    def r2c_ptr(self, field: int, scales: int, stream: int = 0):
+        _check(load_library().gpufft_exec16_r2c(self._h, field, scales, stream))
+
+    def c2r_ptr(self, field: int, scales: int, stream: int = 0):
+        _check(load_library().gpufft_exec16_c2r(self._h, field, scales, stream))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_plan16_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

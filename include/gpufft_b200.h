@@ -150,6 +150,29 @@ int gpufft_batch_status(gpufft_batch batch, void *stream);
 /* Work items per launch. */
 int gpufft_batch_items(gpufft_batch batch);
 
+/* --------------------------------------------------------------------------
+ * Precision form (no counterpart in the reference, which is FP32/FP64 only,
+ * GPU_FFT.h:112-120): the in-place field is stored in 16 bits — format 0 =
+ * BF16, 1 = FP16 — half the bytes of the FP32 form, with one FP32 scale per
+ * pencil; butterflies run in FP32.  `scales` is a device buffer of
+ * gpufft_plan16_scale_count() floats: per z-row scales of the real field
+ * (index x*Ny + y) before R2C / after C2R, per x-pencil scales of the
+ * spectrum (index ky*(Nz/2+1) + kz) after R2C / before C2R.  A stored value
+ * is value/scale with scale = max(|re|,|im|) over its pencil.  Grids with
+ * compiled kernels: cubic powers of two from 64 to 1024.
+ * ------------------------------------------------------------------------ */
+typedef struct gpufft_plan16_s *gpufft_plan16;
+int gpufft_plan16_create(gpufft_plan16 *plan, int64_t nx, int64_t ny, int64_t nz, int format);
+int gpufft_plan16_destroy(gpufft_plan16 plan);
+int64_t gpufft_plan16_scale_count(gpufft_plan16 plan);
+int gpufft_exec16_r2c(gpufft_plan16 plan, void *data, float *scales, void *stream);
+int gpufft_exec16_c2r(gpufft_plan16 plan, void *data, float *scales, void *stream);
+/* FP32 padded real field (Nx*Ny*2*(Nz/2+1) floats) -> 16-bit field + per-row scales. */
+int gpufft_quantize16(gpufft_plan16 plan, const float *field, void *data, float *row_scales, void *stream);
+/* 16-bit field -> FP32 (spectrum != 0: per x-pencil scales; else per z-row scales). */
+int gpufft_dequantize16(gpufft_plan16 plan, const void *data, const float *scales, float *out, int spectrum,
+                        void *stream);
+
 /* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
 int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);
 
