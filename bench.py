@@ -657,6 +657,250 @@ def run_precision(args, world, rank):
     }
 
 
+# ---------------------------------------------------------------------------
+# serving form: Poisson arrivals of mixed requests through the request loop
+# ---------------------------------------------------------------------------
+SERVE_BUDGET = 120 * 10 ** 9   # HBM admission budget (bytes of fields in flight)
+SERVE_16BIT = (64, 96, 128, 192, 256, 384, 512)   # cubic grids with 16-bit kernels
+
+
+def serve_requests(n, seed):
+    """n requests: cubic grids log-uniform over the 2^a*3^b sizes (a >= 1) in
+    [32, 512] (nearest in log), 80% FP32 / 10% BF16 / 10% FP64, R2C or C2R
+    with equal odds.  BF16 requests draw from the sizes with 16-bit kernels."""
+    rng = np.random.default_rng(seed)
+    sizes = sorted({2 ** a * 3 ** b for a in range(1, 10) for b in range(0, 6) if 32 <= 2 ** a * 3 ** b <= 512})
+    out = []
+    for _ in range(n):
+        u = rng.random()
+        prec = "f32" if u < 0.8 else ("bf16" if u < 0.9 else "f64")
+        t = rng.uniform(np.log(32), np.log(512))
+        cand = SERVE_16BIT if prec == "bf16" else sizes
+        nn = min(cand, key=lambda s_: abs(np.log(s_) - t))
+        out.append(((nn, nn, nn), prec, "r2c" if rng.random() < 0.5 else "c2r"))
+    return out, sizes
+
+
+def serve_req_bytes(grid, prec):
+    nx, ny, nz = grid
+    return nx * ny * (nz // 2 + 1) * {"f32": 8, "f64": 16, "bf16": 4}[prec]
+
+
+class FieldPool:
+    """Device-resident fields, `depth` per (grid, precision), reused round robin;
+    a field is handed out again only after its previous request completed."""
+
+    def __init__(self, g, torch, reqs, depth):
+        self.fields = {}
+        self.next = {}
+        self.last = {}
+        count = {}
+        for gr, prec, _ in reqs:
+            count[(gr, prec)] = count.get((gr, prec), 0) + 1
+        for (gr, prec), c in count.items():
+            nx, ny, nz = gr
+            nh = nz // 2 + 1
+            lst = []
+            p16 = g.Plan16(nx, ny, nz, "bf16") if prec == "bf16" else None
+            for k in range(min(depth, c)):
+                gen = torch.Generator(device="cuda").manual_seed(hash((gr, prec, k)) & 0xFFFF)
+                if prec in ("f32", "f64"):
+                    dt = torch.float32 if prec == "f32" else torch.float64
+                    f = torch.zeros((nx, ny, 2 * nh), dtype=dt, device="cuda")
+                    f[:, :, :nz] = torch.randn((nx, ny, nz), generator=gen, dtype=dt, device="cuda")
+                    lst.append((f, None))
+                else:
+                    real = torch.zeros((nx, ny, 2 * nh), device="cuda")
+                    real[:, :, :nz] = torch.randn((nx, ny, nz), generator=gen, device="cuda")
+                    field, scales = p16.empty()
+                    p16.quantize(real, field, scales)
+                    del real
+                    lst.append((field, scales))
+            self.fields[(gr, prec)] = lst
+            self.next[(gr, prec)] = 0
+        torch.cuda.synchronize()
+
+    def reset(self):
+        """Start of a run: request indices restart at 0."""
+        self.last.clear()
+        for k in self.next:
+            self.next[k] = 0
+
+    def take(self, key, i):
+        """(field, scales, index of the request that last used this field)."""
+        k = self.next[key]
+        self.next[key] = (k + 1) % len(self.fields[key])
+        prev = self.last.get((key, k), -1)
+        self.last[(key, k)] = i
+        f, s = self.fields[key][k]
+        return f, s, prev
+
+
+def serve_wait_until(t):
+    while True:
+        d = t - time.perf_counter()
+        if d <= 0:
+            return
+        if d > 3e-4:
+            time.sleep(d - 2e-4)
+
+
+def serve_server_run(g, srv, reqs, arrivals, pool):
+    """Submit each request at its arrival time; a collector thread waits for
+    completions.  Latency = (submit - arrival) + the server's submit-to-done."""
+    n = len(reqs)
+    ids = [0] * n
+    lag = [0.0] * n
+    lat = [0.0] * n
+    done = [False] * n
+    submitted = threading.Semaphore(0)
+    errors = []
+
+    def collector():
+        for i in range(n):
+            submitted.acquire()
+            try:
+                lat[i] = srv.wait(ids[i], 120.0) + lag[i] * 1e3
+            except Exception as e:  # reported by the caller
+                errors.append(repr(e))
+            done[i] = True
+
+    pool.reset()
+    th = threading.Thread(target=collector)
+    th.start()
+    t0 = time.perf_counter() + 0.01
+    for i, (gr, prec, d) in enumerate(reqs):
+        f, s, prev = pool.take((gr, prec), i)
+        while prev >= 0 and not done[prev]:
+            time.sleep(0)
+        serve_wait_until(t0 + arrivals[i])
+        ts = time.perf_counter()
+        ids[i] = srv.submit(srv.request(gr, prec, d, f, s if s is not None else 0))
+        lag[i] = ts - (t0 + arrivals[i])
+        submitted.release()
+    th.join()
+    makespan = time.perf_counter() - t0
+    if errors:
+        raise RuntimeError(errors[0])
+    return lat, makespan, max(lag) * 1e3
+
+
+def serve_serial_run(torch, plans, reqs, arrivals, pool, stream):
+    """Plain serial per-request calls: each request runs alone on one stream
+    and the host waits for it before taking the next one."""
+    n = len(reqs)
+    lat = [0.0] * n
+    pool.reset()
+    t0 = time.perf_counter() + 0.01
+    sh = stream.cuda_stream
+    for i, (gr, prec, d) in enumerate(reqs):
+        f, s, _ = pool.take((gr, prec), i)
+        serve_wait_until(t0 + arrivals[i])
+        p = plans[(gr, prec)]
+        if s is None:
+            (p.r2c_ptr if d == "r2c" else p.c2r_ptr)(f.data_ptr(), sh)
+        else:
+            (p.r2c_ptr if d == "r2c" else p.c2r_ptr)(f.data_ptr(), s.data_ptr(), sh)
+        stream.synchronize()
+        lat[i] = (time.perf_counter() - (t0 + arrivals[i])) * 1e3
+    return lat, time.perf_counter() - t0
+
+
+def serve_errors(g, torch, srv):
+    """Relative L2 error vs FP64 of one served R2C per precision (128^3, N(0,1))."""
+    n = 128
+    gen = torch.Generator(device="cuda").manual_seed(77)
+    real = torch.zeros((n, n, n + 2), dtype=torch.float64, device="cuda")
+    real[:, :, :n] = torch.randn((n, n, n), generator=gen, dtype=torch.float64, device="cuda")
+    ref = real.clone()
+    g.Plan(n, n, n, "double").r2c(ref)
+    out = {}
+    for prec in ("f32", "bf16", "f64"):
+        if prec == "bf16":
+            p16 = g.Plan16(n, n, n, "bf16")
+            field, scales = p16.empty()
+            p16.quantize(real.float(), field, scales)
+            torch.cuda.synchronize()
+            srv.wait(srv.submit(srv.request((n, n, n), prec, "r2c", field, scales)))
+            got = torch.empty((n, n, n + 2), device="cuda")
+            p16.dequantize(field, scales, got, spectrum=True)
+        else:
+            got = real.clone() if prec == "f64" else real.float()
+            torch.cuda.synchronize()
+            srv.wait(srv.submit(srv.request((n, n, n), prec, "r2c", got)))
+        torch.cuda.synchronize()
+        out[prec] = float(((got.double() - ref).norm() / ref.norm()).item())
+    return out
+
+
+def run_serving(args, world, rank):
+    import torch
+    import gpu_fft_b200 as g
+
+    n_req = args.serve_requests
+    slots = args.serve_slots
+    reqs, sizes = serve_requests(n_req, seed=31)
+    pool = FieldPool(g, torch, reqs, depth=slots + 2)
+    srv = g.Server(SERVE_BUDGET, slots)
+    plans = {}
+    for gr, prec, _ in reqs:
+        if (gr, prec) not in plans:
+            srv.prepare(srv.request(gr, prec))
+            plans[(gr, prec)] = (g.Plan16(*gr, "bf16") if prec == "bf16"
+                                 else g.Plan(*gr, "float" if prec == "f32" else "double"))
+    stream = torch.cuda.Stream()
+    total_bytes = sum(serve_req_bytes(gr, p) for gr, p, _ in reqs)
+    # warm-up, then capacity: every request arrives at t = 0
+    zero = [0.0] * n_req
+    serve_serial_run(torch, plans, reqs[: min(200, n_req)], zero, pool, stream)
+    serve_server_run(g, srv, reqs[: min(200, n_req)], zero, pool)
+    _, serial_span = serve_serial_run(torch, plans, reqs, zero, pool, stream)
+    _, server_span, _ = serve_server_run(g, srv, reqs, zero, pool)
+    serial_cap = n_req / serial_span
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0, size=n_req)
+    rows = []
+    sys.setswitchinterval(1e-4)
+    for load in args.serve_loads:
+        rate = load * serial_cap
+        arr = list(np.cumsum(gaps / rate) - gaps[0] / rate)
+        lat_s, span_s, max_lag = serve_server_run(g, srv, reqs, arr, pool)
+        lat_q, span_q = serve_serial_run(torch, plans, reqs, arr, pool, stream)
+        rows.append({
+            "load_vs_serial_capacity": load, "rate_rps": round(rate, 1),
+            "server": {"p50_ms": round(pct(lat_s, 50), 4), "p99_ms": round(pct(lat_s, 99), 4),
+                       "mean_ms": round(statistics.mean(lat_s), 4), "throughput_rps": round(n_req / span_s, 1),
+                       "field_gbs": round(total_bytes / span_s / 1e9, 1), "max_submit_lag_ms": round(max_lag, 3)},
+            "serial": {"p50_ms": round(pct(lat_q, 50), 4), "p99_ms": round(pct(lat_q, 99), 4),
+                       "mean_ms": round(statistics.mean(lat_q), 4), "throughput_rps": round(n_req / span_q, 1),
+                       "field_gbs": round(total_bytes / span_q / 1e9, 1)},
+        })
+    sys.setswitchinterval(5e-3)
+    errs = serve_errors(g, torch, srv)
+    st = srv.stats()
+    srv.close()
+    if rank != 0:
+        return None
+    head = min(rows, key=lambda r: abs(r["load_vs_serial_capacity"] - 0.8))
+    mix = {p: sum(1 for _, q, _ in reqs if q == p) for p in ("f32", "bf16", "f64")}
+    return {
+        "metric": "serving form: p99 request latency at 80% of the serial loop's capacity (Poisson arrivals)",
+        "value": head["server"]["p99_ms"], "unit": "ms", "n_gpus": world, "steps": n_req, "warmup": min(200, n_req),
+        "ms_per_step": head["server"]["mean_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 / bf16 storage / f64 mix",
+        "data": "synthetic: seeded N(0,1) fields, device-resident, reused round robin",
+        "config": {"workload": "serving", "requests": n_req, "slots": slots, "hbm_budget_bytes": SERVE_BUDGET,
+                   "grid_sizes": sizes, "bf16_sizes": list(SERVE_16BIT), "mix": mix,
+                   "directions": {d: sum(1 for *_, e in reqs if e == d) for d in ("r2c", "c2r")},
+                   "total_field_bytes": total_bytes},
+        "capacity": {"serial_rps": round(serial_cap, 1), "server_rps": round(n_req / server_span, 1),
+                     "speedup": round(serial_span / server_span, 3)},
+        "loads": rows,
+        "errors_vs_fp64_rel_l2": errs,
+        "server_stats": {k: st[k] for k in ("completed", "failed", "max_in_flight", "peak_bytes_in_use", "plans")},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -669,8 +913,13 @@ def main():
     ap.add_argument("--dtype", choices=["float", "double"], default=DTYPE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the default kernel candidates")
-    ap.add_argument("--workload", choices=["headline", "batch64", "spectral", "precision"], default="headline",
-                    help="headline: 512^3 R2C+C2R (the bench contract); batch64 / spectral: batched form")
+    ap.add_argument("--workload", choices=["headline", "batch64", "spectral", "precision", "serving"],
+                    default="headline",
+                    help="headline: 512^3 R2C+C2R (the bench contract); batch64 / spectral: batched form; "
+                         "precision: 16-bit storage form at 1024^3; serving: request loop under Poisson arrivals")
+    ap.add_argument("--serve-requests", type=int, default=3000)
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.8, 1.0, 1.5, 2.5])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -680,6 +929,8 @@ def main():
             res = run_batch(args, world, rank)
         elif args.workload == "precision":
             res = run_precision(args, world, rank)
+        elif args.workload == "serving":
+            res = run_serving(args, world, rank)
         elif args.impl == "reference":
             res = run_reference(args, world, rank)
         else:

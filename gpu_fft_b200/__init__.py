@@ -21,7 +21,8 @@ LIB_PATH = os.path.join(_HERE, "libgpufft_b200.so")
 
 GPUFFT_FLOAT = 0
 GPUFFT_DOUBLE = 1
-STATUS = {0: "SUCCESS", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NOT_INIT", 5: "ERR_OOM"}
+STATUS = {0: "SUCCESS", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NOT_INIT", 5: "ERR_OOM",
+          6: "ERR_TIMEOUT", 7: "ERR_CANCELLED"}
 
 # every symbol include/gpufft_b200.h declares
 EXPORTS = (
@@ -34,10 +35,27 @@ EXPORTS = (
     "gpufft_batch_status", "gpufft_batch_items",
     "gpufft_plan16_create", "gpufft_plan16_destroy", "gpufft_plan16_scale_count", "gpufft_exec16_r2c",
     "gpufft_exec16_c2r", "gpufft_quantize16", "gpufft_dequantize16",
+    "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
+    "gpufft_server_submit", "gpufft_server_poll", "gpufft_server_wait", "gpufft_server_cancel", "gpufft_server_stats",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 
 _lib = None
+
+
+class Request(ctypes.Structure):
+    """gpufft_request"""
+    _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("nz", ctypes.c_int64), ("precision", ctypes.c_int),
+                ("direction", ctypes.c_int), ("data", ctypes.c_void_p), ("scales", ctypes.c_void_p),
+                ("ready_event", ctypes.c_void_p)]
+
+
+class ServerStats(ctypes.Structure):
+    """gpufft_server_stats_t"""
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("cancelled", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("in_flight", ctypes.c_int64), ("max_in_flight", ctypes.c_int64),
+                ("bytes_in_use", ctypes.c_int64), ("peak_bytes_in_use", ctypes.c_int64), ("plans", ctypes.c_int64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double)]
 
 
 class GpuFFTError(RuntimeError):
@@ -88,6 +106,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_exec16_c2r.argtypes = [vp, vp, vp, vp]
     lib.gpufft_quantize16.argtypes = [vp, vp, vp, vp, vp]
     lib.gpufft_dequantize16.argtypes = [vp, vp, vp, vp, ci, vp]
+    rp = ctypes.POINTER(Request)
+    lib.gpufft_server_create.argtypes = [ctypes.POINTER(vp), i64, ci, ci]
+    lib.gpufft_server_stop.argtypes = [vp]
+    lib.gpufft_server_destroy.argtypes = [vp]
+    lib.gpufft_server_prepare.argtypes = [vp, rp]
+    lib.gpufft_server_submit.argtypes = [vp, rp, ctypes.POINTER(i64)]
+    lib.gpufft_server_poll.argtypes = [vp, i64, ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_double)]
+    lib.gpufft_server_wait.argtypes = [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    lib.gpufft_server_cancel.argtypes = [vp, i64]
+    lib.gpufft_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
     for name in EXPORTS:
         if getattr(lib, name, None) is None:
             raise ImportError(f"{path} does not export {name}")
@@ -307,6 +335,72 @@ class Plan16:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().gpufft_plan16_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+PRECISIONS = {"f32": 0, "float": 0, "f64": 1, "double": 1, "bf16": 2, "fp16": 3}
+REQ_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class Server:
+    """Continuous-batching request loop (gpufft_server_*): submit R2C / C2R
+    requests on device-resident fields; they are admitted as stream slots and
+    the HBM budget free up and run concurrently."""
+
+    def __init__(self, budget_bytes: int, slots: int = 8, dryrun: bool = False):
+        h = ctypes.c_void_p()
+        _check(load_library().gpufft_server_create(ctypes.byref(h), int(budget_bytes), int(slots), 1 if dryrun else 0))
+        self._h = h
+
+    @staticmethod
+    def request(grid, precision="f32", direction="r2c", data=0, scales=0, ready_event=0) -> Request:
+        """A request on a device field (pointer or tensor).  ready_event: a
+        torch.cuda.Event (or raw cudaEvent_t) recorded after the field was
+        written; without one the field must be complete when submitted."""
+        nx, ny, nz = grid
+        ptr = lambda x: x.data_ptr() if hasattr(x, "data_ptr") else int(x or 0)
+        ev = ready_event.cuda_event if hasattr(ready_event, "cuda_event") else int(ready_event or 0)
+        return Request(int(nx), int(ny), int(nz), PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                       1 if direction in ("r2c", 1, True) else 0, ptr(data) or None, ptr(scales) or None, ev or None)
+
+    def prepare(self, req: Request) -> None:
+        _check(load_library().gpufft_server_prepare(self._h, ctypes.byref(req)))
+
+    def submit(self, req: Request) -> int:
+        rid = ctypes.c_int64()
+        _check(load_library().gpufft_server_submit(self._h, ctypes.byref(req), ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int):
+        st, lat = ctypes.c_int(), ctypes.c_double()
+        _check(load_library().gpufft_server_poll(self._h, rid, ctypes.byref(st), ctypes.byref(lat)))
+        return REQ_STATUS[st.value], lat.value
+
+    def wait(self, rid: int, timeout_s: float = 30.0) -> float:
+        lat = ctypes.c_double()
+        _check(load_library().gpufft_server_wait(self._h, rid, float(timeout_s), ctypes.byref(lat)))
+        return lat.value
+
+    def cancel(self, rid: int) -> None:
+        _check(load_library().gpufft_server_cancel(self._h, rid))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(load_library().gpufft_server_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def stop(self) -> None:
+        _check(load_library().gpufft_server_stop(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -215,7 +215,7 @@ static int batch_configure(Batch &B) {
             if (round == 0 && pass == 1 && P.nx == 1) B.hdesc[t].n_first = 0;  // nothing to wait for
         }
     B.smem = smem_elems * sizeof(V);
-    cudaError_t e = cudaFuncSetAttribute(batch_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem);
+    cudaError_t e = raise_smem_limit((const void *)batch_kernel<T>, B.smem);
     if (e != cudaSuccess)
         return set_error(GPUFFT_ERR_UNSUPPORTED, "batch needs %zu bytes of shared memory: %s", B.smem,
                          cudaGetErrorString(e));

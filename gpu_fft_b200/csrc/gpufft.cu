@@ -34,6 +34,20 @@ namespace gpufft {
 // ---------------------------------------------------------------------------
 static thread_local std::string g_last_error;
 
+cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &cur = limit[std::make_pair(dev, fn)];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 int set_error(int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
@@ -224,7 +238,7 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         if (vb[i].nx == nx && (vb[i].kind == 0 || rows16) && seen++ == idx_b) P.fb = &vb[i];
     if (P.fa) {
         for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.fa->smem);
+            cudaError_t e = raise_smem_limit(k, P.fa->smem);
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 P.fa = nullptr;
@@ -253,7 +267,7 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
     }
     if (P.fb) {
         for (const void *k : {P.fb->kfwd, P.fb->kinv}) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.fb->smem);
+            cudaError_t e = raise_smem_limit(k, P.fb->smem);
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 P.fb = nullptr;
@@ -515,12 +529,12 @@ static int build_plan(Plan &P) {
     auto ka_f = pass_a_kernel<T, true>, ka_i = pass_a_kernel<T, false>;
     auto kb_f = pass_b_kernel<T, true>, kb_i = pass_b_kernel<T, false>;
     for (auto k : {ka_f, ka_i}) {
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_a);
+        e = raise_smem_limit((const void *)k, P.smem_a);
         if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(pass A smem)");
         cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     }
     for (auto k : {kb_f, kb_i}) {
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_b);
+        e = raise_smem_limit((const void *)k, P.smem_b);
         if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(pass B smem)");
     }
     const int sms = device_sms(P.device);

@@ -4,6 +4,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "fast_registry.h"
 #include "fft_kernels.cuh"
 
@@ -30,6 +32,10 @@ struct Plan {
 
 int set_error(int code, const char *fmt, ...);
 const char *last_error();
+// Raises a kernel's dynamic shared memory limit on the current device to at
+// least `bytes`.  Never lowers it: plans of different sizes share the generic
+// kernels, and a later, smaller plan must not undo an earlier plan's limit.
+cudaError_t raise_smem_limit(const void *fn, size_t bytes);
 int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
 int plan_destroy(Plan *P);
 int plan_exec(const Plan *P, void *data, void *stream, bool forward);

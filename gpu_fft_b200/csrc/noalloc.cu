@@ -151,8 +151,8 @@ int exec_noalloc(int nx, int ny, int nz, bool forward, void *data, cudaStream_t 
 
     const void *ka = forward ? (const void *)pass_a_kernel<T, true> : (const void *)pass_a_kernel<T, false>;
     const void *kb = forward ? (const void *)pass_b_kernel<T, true> : (const void *)pass_b_kernel<T, false>;
-    e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b);
+    e = raise_smem_limit(ka, smem_a);
+    if (e == cudaSuccess) e = raise_smem_limit(kb, smem_b);
     if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "kernel attributes: %s", cudaGetErrorString(e));
     int sms = 0, occ_b = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -37,14 +37,18 @@ struct VarB {
 static const VarA kA[] = {
     S16_A(0, 1024, 512, 1, 8, 256, 2), S16_A(1, 1024, 512, 1, 8, 256, 2),
     S16_A(0, 512, 256, 2, 8, 256, 2),  S16_A(1, 512, 256, 2, 8, 256, 2),
+    S16_A(0, 384, 192, 1, 8, 256, 1),  S16_A(1, 384, 192, 1, 8, 256, 1),
     S16_A(0, 256, 128, 2, 8, 256, 2),  S16_A(1, 256, 128, 2, 8, 256, 2),
+    S16_A(0, 192, 96, 1, 8, 256, 2),   S16_A(1, 192, 96, 1, 8, 256, 2),
     S16_A(0, 128, 64, 4, 8, 256, 2),   S16_A(1, 128, 64, 4, 8, 256, 2),
+    S16_A(0, 96, 48, 2, 8, 256, 2),    S16_A(1, 96, 48, 2, 8, 256, 2),
     S16_A(0, 64, 32, 4, 8, 256, 2),    S16_A(1, 64, 32, 4, 8, 256, 2),
 };
 static const VarB kB[] = {
     S16_B(0, 1024, 8, 256, 2), S16_B(1, 1024, 8, 256, 2), S16_B(0, 512, 16, 256, 2), S16_B(1, 512, 16, 256, 2),
     S16_B(0, 256, 16, 256, 2), S16_B(1, 256, 16, 256, 2), S16_B(0, 128, 16, 256, 2), S16_B(1, 128, 16, 256, 2),
-    S16_B(0, 64, 16, 256, 2),  S16_B(1, 64, 16, 256, 2),
+    S16_B(0, 64, 16, 256, 2),  S16_B(1, 64, 16, 256, 2),  S16_B(0, 384, 8, 256, 2),  S16_B(1, 384, 8, 256, 2),
+    S16_B(0, 192, 16, 256, 2), S16_B(1, 192, 16, 256, 2), S16_B(0, 96, 16, 256, 2),  S16_B(1, 96, 16, 256, 2),
 };
 
 struct Plan16 {
@@ -101,8 +105,8 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
         if (v.fmt == fmt && v.nx == nx) { vb = &v; break; }
     if (!va || !vb)
         return set_error(GPUFFT_ERR_UNSUPPORTED,
-                         "16-bit storage form: grid %lldx%lldx%lld has no compiled kernels (cubic 64..1024 powers "
-                         "of two are built)", (long long)nx, (long long)ny, (long long)nz);
+                         "16-bit storage form: grid %lldx%lldx%lld has no compiled kernels (cubic 64, 96, 128, "
+                         "192, 256, 384, 512 and 1024 are built)", (long long)nx, (long long)ny, (long long)nz);
     Plan16 *P = new (std::nothrow) Plan16();
     if (!P) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
     P->nx = nx; P->ny = ny; P->nz = nz; P->fmt = fmt; P->va = va; P->vb = vb;
@@ -139,9 +143,9 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
     P->sty = tb + oy;
     P->stw = tb + ox;
     for (const void *k : {va->kfwd, va->kinv})
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)va->smem);
+        if (e == cudaSuccess) e = raise_smem_limit(k, va->smem);
     for (const void *k : {vb->kfwd, vb->kinv})
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vb->smem);
+        if (e == cudaSuccess) e = raise_smem_limit(k, vb->smem);
     if (e != cudaSuccess) {
         plan16_free(P);
         return set_error(GPUFFT_ERR_CUDA, "16-bit plan set-up: %s", cudaGetErrorString(e));

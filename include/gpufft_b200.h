@@ -40,7 +40,9 @@ typedef enum {
     GPUFFT_ERR_UNSUPPORTED = 2,  /* valid but not handled (procs > 1, odd Nz, prime factor > 13, axis too long) */
     GPUFFT_ERR_CUDA = 3,         /* a CUDA runtime call failed */
     GPUFFT_ERR_NOT_INIT = 4,     /* no plan for this dtype: call gpufft_init first */
-    GPUFFT_ERR_OOM = 5           /* device allocation failed */
+    GPUFFT_ERR_OOM = 5,          /* device allocation failed, or a request larger than a server's budget */
+    GPUFFT_ERR_TIMEOUT = 6,      /* a bounded wait ran out */
+    GPUFFT_ERR_CANCELLED = 7     /* the request was cancelled before it started */
 } gpufft_status;
 
 typedef struct gpufft_plan_s *gpufft_plan;
@@ -172,6 +174,54 @@ int gpufft_quantize16(gpufft_plan16 plan, const float *field, void *data, float 
 /* 16-bit field -> FP32 (spectrum != 0: per x-pencil scales; else per z-row scales). */
 int gpufft_dequantize16(gpufft_plan16 plan, const void *data, const float *scales, float *out, int spectrum,
                         void *stream);
+
+/* --------------------------------------------------------------------------
+ * Serving: a continuous-batching request loop (no counterpart in the
+ * reference, which is one call per transform, FFT_R2C.cu:41-70).  Plans,
+ * twiddle tables and fields stay resident on the device; a dispatcher thread
+ * admits queued requests as stream slots and HBM budget free up, runs them
+ * concurrently on its streams and reports latency from submit to completion.
+ * ------------------------------------------------------------------------ */
+typedef enum { GPUFFT_REQ_F32 = 0, GPUFFT_REQ_F64 = 1, GPUFFT_REQ_BF16 = 2, GPUFFT_REQ_FP16 = 3 } gpufft_req_precision;
+typedef enum {
+    GPUFFT_REQ_QUEUED = 0,
+    GPUFFT_REQ_RUNNING = 1,
+    GPUFFT_REQ_DONE = 2,
+    GPUFFT_REQ_FAILED = 3,
+    GPUFFT_REQ_CANCELLED = 4
+} gpufft_req_status;
+typedef struct {
+    int64_t nx, ny, nz;
+    int precision;   /* gpufft_req_precision */
+    int direction;   /* 1 = R2C, 0 = C2R */
+    void *data;         /* device field, in place */
+    float *scales;      /* per-pencil scales (16-bit precisions only) */
+    void *ready_event;  /* cudaEvent_t the transform waits for (the producer of
+                           the field recorded it), or NULL if the field is
+                           already complete when submitted */
+} gpufft_request;
+typedef struct {
+    int64_t completed, failed, cancelled, queued, in_flight, max_in_flight;
+    int64_t bytes_in_use, peak_bytes_in_use, plans;
+    double p50_ms, p99_ms;
+} gpufft_server_stats_t;
+typedef struct gpufft_server_s *gpufft_server;
+#define GPUFFT_SERVER_DRYRUN 1 /* host timers instead of the GPU (tests of the scheduling) */
+
+/* budget_bytes: sum of the field bytes of admitted requests; slots: requests
+ * in flight at once (one CUDA stream each). */
+int gpufft_server_create(gpufft_server *server, int64_t budget_bytes, int slots, int flags);
+/* Stops admitting, lets requests in flight finish, fails those still queued. */
+int gpufft_server_stop(gpufft_server server);
+int gpufft_server_destroy(gpufft_server server);
+/* Builds the plan a request of this shape and precision will use. */
+int gpufft_server_prepare(gpufft_server server, const gpufft_request *request);
+int gpufft_server_submit(gpufft_server server, const gpufft_request *request, int64_t *id);
+int gpufft_server_poll(gpufft_server server, int64_t id, int *status, double *latency_ms);
+/* Bounded wait: GPUFFT_ERR_TIMEOUT after timeout_s seconds. */
+int gpufft_server_wait(gpufft_server server, int64_t id, double timeout_s, double *latency_ms);
+int gpufft_server_cancel(gpufft_server server, int64_t id);
+int gpufft_server_stats(gpufft_server server, gpufft_server_stats_t *stats);
 
 /* Bytes of the in-place field: Nx*Ny*(Nz/2+1)*sizeof(complex). */
 int64_t gpufft_field_bytes(int64_t nx, int64_t ny, int64_t nz, int dtype);

@@ -242,6 +242,25 @@ def test_plans_coexist_and_singletons_per_dtype(oracle, cuda):
         g.GPU_FFT_R2C(torch.zeros(8, 8, 10, device="cuda"))
 
 
+@pytest.mark.parametrize("dt", ["float", "double"])
+def test_smaller_plan_created_later_keeps_larger_plan_working(oracle, cuda, dt):
+    """Plans share the generic kernels; creating a plan that needs less shared
+    memory must not lower the limit an existing, larger plan launches with."""
+    import torch
+    import gpu_fft_b200 as g
+
+    big = g.Plan(90, 96, 108, dt)
+    small = g.Plan(20, 18, 12, dt)
+    for grid, p in (((20, 18, 12), small), ((90, 96, 108), big)):
+        f = oracle.uniform_field(*grid, seed=4, dtype=NPDT[dt])
+        d = torch.from_numpy(f.copy()).cuda()
+        p.r2c(d)
+        torch.cuda.synchronize()
+        cdt = np.complex64 if dt == "float" else np.complex128
+        got = d.cpu().numpy().view(cdt).reshape(grid[0], grid[1], grid[2] // 2 + 1)
+        assert oracle.rel_l2(got, oracle.c_r2c(f.astype(np.float64), *grid)) < TOL[dt]
+
+
 def test_unsupported_and_invalid_on_gpu(cuda):
     import torch
     import gpu_fft_b200 as g

@@ -11,7 +11,7 @@ BAR = {"fp16": 1e-3, "bf16": 6e-3}
 
 
 @pytest.mark.parametrize("fmt", ["fp16", "bf16"])
-@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("n", [64, 96, 128, 192, 256, 384])
 def test_r2c_c2r_16bit_against_oracle(oracle, cuda, fmt, n):
     import torch
     import gpu_fft_b200 as g
@@ -64,5 +64,5 @@ def test_16bit_rejects_grids_without_kernels(cuda):
     import gpu_fft_b200 as g
 
     with pytest.raises(g.GpuFFTError) as e:
-        g.Plan16(96, 96, 96)
+        g.Plan16(160, 160, 160)
     assert e.value.code == 2
