@@ -480,30 +480,43 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
                 }
             } else {
                 // pre-process: Z[k] = S + Pk, Z[m-k] = conj(S - Pk), S = X[k] + conj X[m-k],
-                // Pk = i conj(w^k)(X[k] - conj X[m-k]); slot 0 holds (Re X0, Re Xm)
-                __syncwarp();
+                // Pk = i conj(w^k)(X[k] - conj X[m-k]); slot 0 holds (Re X0, Re Xm).
+                // All loads of the warp's rows are issued before any use, so their
+                // latencies overlap instead of adding up.
+                constexpr int KPL = (HALF + 31) / 32;
+                V xk[RW][KPL], xm[RW][KPL];
+#pragma unroll
                 for (int w = 0; w < RW; ++w) {
                     const V *row = gr + (long long)w * NH;
-                    for (int k = lane; k < HALF; k += 32) {
-                        V za = V{(T)0, (T)0}, zb = V{(T)0, (T)0};
-                        if (w < wv) {
-                            V xk, xmk;
-                            if (k == 0) {
-                                const V pk = ld_g(row);
-                                xk = V{pk.x, (T)0};
-                                xmk = V{pk.y, (T)0};
-                            } else {
-                                xk = ld_g(row + k);
-                                xmk = ld_g(row + M - k);
-                            }
-                            const V cm = c_conj(xmk);
-                            const V s = c_add(xk, cm);
-                            const V pk = c_rot<false>(c_mulc(c_sub(xk, cm), unp[k]));
-                            za = c_add(s, pk);
-                            zb = c_conj(c_sub(s, pk));
+#pragma unroll
+                    for (int u = 0; u < KPL; ++u) {
+                        const int k = lane + 32 * u;
+                        xk[w][u] = V{(T)0, (T)0};
+                        xm[w][u] = V{(T)0, (T)0};
+                        if (w < wv && k < HALF) {
+                            xk[w][u] = ld_g(row + k);
+                            if (k != 0) xm[w][u] = ld_g(row + M - k);
                         }
-                        wtile[RowL::idx(k, w)] = za;
-                        if (k != 0 && M - k != k) wtile[RowL::idx(M - k, w)] = zb;
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int w = 0; w < RW; ++w) {
+#pragma unroll
+                    for (int u = 0; u < KPL; ++u) {
+                        const int k = lane + 32 * u;
+                        if (k < HALF) {
+                            V a = xk[w][u], b = xm[w][u];
+                            if (k == 0) {
+                                b = V{a.y, (T)0};
+                                a = V{a.x, (T)0};
+                            }
+                            const V cm = c_conj(b);
+                            const V s = c_add(a, cm);
+                            const V pk = c_rot<false>(c_mulc(c_sub(a, cm), unp[k]));
+                            wtile[RowL::idx(k, w)] = c_add(s, pk);
+                            if (k != 0 && M - k != k) wtile[RowL::idx(M - k, w)] = c_conj(c_sub(s, pk));
+                        }
                     }
                 }
                 auto dst = [&](int n, int w, V v) {
