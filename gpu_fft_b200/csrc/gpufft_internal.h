@@ -27,6 +27,7 @@ struct Plan {
     const fast::VariantB *fb = nullptr;
     int grid_fa = 0, grid_fb = 0, k_fa = 1, occ_fa = 0, occ_fb = 0;
     int idx_a = 0, idx_b = 0;  // registry candidate in use per pass (-1 = generic kernels)
+    int kdiv = 1;              // specialised Pass A cluster size = the chosen size / kdiv
     bool tuned = false;
 };
 
