@@ -303,8 +303,15 @@ def run_ours(args, world, rank):
     dom = max(kmean, key=kmean.get)
     peak, peak_kind = load_peaks()
     achieved = 2 * S / (kmean[dom] * 1e-3) / 1e9
+    # DRAM bytes (read + write) per launch of the dominant kernel from the ncu
+    # capture summarised in profiles/pass_a_fast_512cubed_f32.md; reported
+    # only when this run uses the same kernel configuration
+    traffic = None
+    if (nx, ny, nz, dt) == (512, 512, 512, "float") and dom == "pass_A_fwd" and \
+            "fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4" in plan.describe():
+        traffic = 558_529_024 + 766_980_864
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "kernel": dom,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
                 "algorithmic_bytes_per_launch": 2 * S, "peak_source": peak_kind,
                 "kernel_ms": {k: round(v, 4) for k, v in kmean.items()}}
     step_bytes = 8 * S  # 2 transforms x (2 passes x (read + write) of S)

@@ -252,8 +252,9 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         P.occ_fa = std::max(occ, 1);
         const size_t plane = (size_t)ny * (m + 1) * vs;
         int K = choose_cluster(P.device, nx, ny, m, P.fa->wy, plane, P.occ_fa, sms);
-        // the autotuner may halve the cluster: more planes in flight, each
-        // cluster barrier spanning fewer CTAs (measured up to 3% faster at 512^3)
+        // the autotuner may divide the cluster size by 2 or 4: more planes in
+        // flight, each cluster barrier spanning fewer CTAs (at 512^3 FP32 the
+        // tuner takes K = 4 over 8)
         if (P.kdiv > 1) K = std::max(1, K / P.kdiv);
         if (P.fa->kind == 1) {
             // the plane lives in the cluster's shared memory: the cluster size is fixed
@@ -326,7 +327,7 @@ static int wisdom_load_locked(const char *path) {
         int dt, a, b, kdiv = 1;
         long long nx, ny, nz;
         if (ss >> dev >> dt >> nx >> ny >> nz >> a >> b) {
-            if (!(ss >> kdiv) || (kdiv != 1 && kdiv != 2)) kdiv = 1;  // older files have no divisor
+            if (!(ss >> kdiv) || (kdiv != 1 && kdiv != 2 && kdiv != 4)) kdiv = 1;  // older files have none
             g_wisdom[WisdomKey(dev, dt, nx, ny, nz)] = {a, b, kdiv};
         }
     }
@@ -439,8 +440,8 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
         const int n = count_candidates(*P, pass);
         float best_ms = 1e30f;
         for (int c = -1; c < n; ++c) {
-            // Pass A candidates are timed at the chosen cluster size and at half of it
-            for (int kdiv = 1; kdiv <= (pass == 0 && c >= 0 ? 2 : 1); ++kdiv) {
+            // Pass A candidates are timed at the chosen cluster size, half and a quarter of it
+            for (int kdiv = 1; kdiv <= (pass == 0 && c >= 0 ? 4 : 1); kdiv *= 2) {
                 P->kdiv = pass == 0 ? kdiv : best_kdiv;
                 if (pass == 0)
                     setup_fast(*P, c, P->idx_b);
