@@ -537,21 +537,26 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     // measured slower at 512^3: two planes per cluster in flight overflow L2.
     // Block barriers separate the warp-private row tiles from the shared
     // column tile, which overlap in shared memory.
+    // A split Pass A (P.phases 1 or 2, for planes too large to stay in L2
+    // while a cluster works on them) runs one of the two phases per launch.
+    const bool do_rows = P.phases != 2, do_cols = P.phases != 1;
     for (int plane = cid; plane < P.nx; plane += ncl) {
         V *g = base + (long long)plane * NY * NH;
-        if (FWD)
-            rows(g);
-        else
+        if (FWD) {
+            if (do_rows) rows(g);
+        } else if (do_cols) {
             cols(g);
+        }
         __syncthreads();
-        if (K > 1) {
+        if (K > 1 && P.phases == 0) {
             cluster_arrive();
             cluster_wait();
         }
-        if (FWD)
-            cols(g);
-        else
+        if (FWD) {
+            if (do_cols) cols(g);
+        } else if (do_rows) {
             rows(g);
+        }
         __syncthreads();
     }
 }

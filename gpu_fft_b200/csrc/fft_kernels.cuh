@@ -68,6 +68,11 @@ struct PassAParams {
     AxisPlan az;  // n = Nz/2, tabmul 2
     AxisPlan ay;  // n = Ny, tabmul 1
     int tile_elems;  // complex elements reserved for the tile
+    // specialised kernels: 0 = both axes per plane (cluster barrier between),
+    // 1 = z rows only, 2 = y columns only (the two halves of a split Pass A,
+    // launched one after the other without clusters; K then only splits the
+    // work of a plane between CTAs)
+    int phases;
 };
 
 struct PassBParams {

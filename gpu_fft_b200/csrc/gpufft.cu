@@ -235,7 +235,7 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
     seen = 0;
     const bool rows16 = ((long long)ny * (m + 1) * vs) % 16 == 0;  // cp.async tiles need 16-byte row starts
     for (int i = 0; i < nb && !P.fb; ++i)
-        if (vb[i].nx == nx && (vb[i].kind == 0 || rows16) && seen++ == idx_b) P.fb = &vb[i];
+        if (vb[i].nx == nx && (vb[i].kind != 1 || rows16) && seen++ == idx_b) P.fb = &vb[i];
     if (P.fa) {
         for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
             cudaError_t e = raise_smem_limit(k, P.fa->smem);
@@ -252,22 +252,37 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         P.occ_fa = std::max(occ, 1);
         const size_t plane = (size_t)ny * (m + 1) * vs;
         int K = choose_cluster(P.device, nx, ny, m, P.fa->wy, plane, P.occ_fa, sms);
-        // the autotuner may divide the cluster size by 2 or 4: more planes in
-        // flight, each cluster barrier spanning fewer CTAs (at 512^3 FP32 the
-        // tuner takes K = 4 over 8)
-        if (P.kdiv > 1) K = std::max(1, K / P.kdiv);
-        if (P.fa->kind == 1) {
-            // the plane lives in the cluster's shared memory: the cluster size is fixed
-            K = P.fa->k;
+        // the autotuner may set the cluster size: smaller clusters put more
+        // planes in flight with shorter barriers (512^3 FP32 takes 4 over 8),
+        // 16-CTA clusters (non-portable) put fewer in flight when planes are
+        // large (1024^2)
+        if (P.kfix > 0 && P.fa->kind == 0) {
+            K = std::min(P.kfix, std::max(1, ny));
             if (K > 8) {
                 cudaFuncSetAttribute(P.fa->kfwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
                 cudaFuncSetAttribute(P.fa->kinv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             }
         }
-        const int mc = max_clusters(P.fa->kfwd, K, nx, P.fa->smem, P.fa->nt, std::max(1, P.occ_fa * sms / K));
-        P.k_fa = K;
-        P.grid_fa = K * std::min(nx, mc);
-        if (P.fa->kind == 1 && mc < 1) P.fa = nullptr;
+        // split Pass A: z rows and y columns as two plain launches (the plane
+        // goes through DRAM between them); K CTAs still share each plane
+        P.split_a = P.kfix == -1 && P.fa->kind == 0;
+        if (P.split_a) {
+            P.k_fa = K;
+            P.grid_fa = K * std::max(1, std::min(nx, P.occ_fa * sms / K));
+        } else {
+            if (P.fa->kind == 1) {
+                // the plane lives in the cluster's shared memory: the cluster size is fixed
+                K = P.fa->k;
+                if (K > 8) {
+                    cudaFuncSetAttribute(P.fa->kfwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                    cudaFuncSetAttribute(P.fa->kinv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                }
+            }
+            const int mc = max_clusters(P.fa->kfwd, K, nx, P.fa->smem, P.fa->nt, std::max(1, P.occ_fa * sms / K));
+            P.k_fa = K;
+            P.grid_fa = K * std::min(nx, mc);
+            if (P.fa->kind == 1 && mc < 1) P.fa = nullptr;
+        }
     }
     if (P.fb) {
         for (const void *k : {P.fb->kfwd, P.fb->kinv}) {
@@ -297,7 +312,7 @@ namespace {
 using WisdomKey = std::tuple<std::string, int, long long, long long, long long>;
 std::mutex g_wisdom_mu;
 struct WisdomEntry {
-    int a, b, kdiv;  // Pass A candidate, Pass B candidate, Pass A cluster divisor
+    int a, b, k;  // Pass A candidate, Pass B candidate, Pass A cluster size (0: chosen from L2)
 };
 std::map<WisdomKey, WisdomEntry> g_wisdom;
 bool g_wisdom_env_loaded = false;
@@ -324,11 +339,11 @@ static int wisdom_load_locked(const char *path) {
         if (line.empty() || line[0] == '#') continue;
         std::istringstream ss(line);
         std::string dev;
-        int dt, a, b, kdiv = 1;
+        int dt, a, b, k = 0;
         long long nx, ny, nz;
         if (ss >> dev >> dt >> nx >> ny >> nz >> a >> b) {
-            if (!(ss >> kdiv) || (kdiv != 1 && kdiv != 2 && kdiv != 4)) kdiv = 1;  // older files have none
-            g_wisdom[WisdomKey(dev, dt, nx, ny, nz)] = {a, b, kdiv};
+            if (!(ss >> k) || k < -1 || k > 16 || (k > 0 && (k & (k - 1)))) k = 0;  // older files have none
+            g_wisdom[WisdomKey(dev, dt, nx, ny, nz)] = {a, b, k};
         }
     }
     return GPUFFT_SUCCESS;
@@ -337,11 +352,11 @@ static int wisdom_load_locked(const char *path) {
 static int wisdom_save_locked(const char *path) {
     std::ofstream out(path);
     if (!out) return set_error(GPUFFT_ERR_INVALID, "cannot write wisdom file %s", path);
-    out << "# gpufft_b200 wisdom: device dtype nx ny nz passA_candidate passB_candidate passA_cluster_divisor\n";
+    out << "# gpufft_b200 wisdom: device dtype nx ny nz passA_candidate passB_candidate passA_cluster_size(0=auto,-1=split)\n";
     for (const auto &kv : g_wisdom)
         out << std::get<0>(kv.first) << " " << std::get<1>(kv.first) << " " << std::get<2>(kv.first) << " "
             << std::get<3>(kv.first) << " " << std::get<4>(kv.first) << " " << kv.second.a << " " << kv.second.b << " "
-            << kv.second.kdiv << "\n";
+            << kv.second.k << "\n";
     return GPUFFT_SUCCESS;
 }
 
@@ -355,7 +370,7 @@ int wisdom_load(const char *path) {
     return wisdom_load_locked(path);
 }
 
-static bool wisdom_lookup(const Plan &P, int &ia, int &ib, int &kdiv) {
+static bool wisdom_lookup(const Plan &P, int &ia, int &ib, int &k) {
     std::lock_guard<std::mutex> lk(g_wisdom_mu);
     if (!g_wisdom_env_loaded) {
         g_wisdom_env_loaded = true;
@@ -369,13 +384,13 @@ static bool wisdom_lookup(const Plan &P, int &ia, int &ib, int &kdiv) {
     if (it == g_wisdom.end()) return false;
     ia = it->second.a;
     ib = it->second.b;
-    kdiv = it->second.kdiv;
+    k = it->second.k;
     return true;
 }
 
 static void wisdom_store(const Plan &P) {
     std::lock_guard<std::mutex> lk(g_wisdom_mu);
-    g_wisdom[wisdom_key(P)] = {P.idx_a, P.idx_b, P.kdiv};
+    g_wisdom[wisdom_key(P)] = {P.idx_a, P.idx_b, P.kfix};
     const char *path = std::getenv("GPUFFT_WISDOM");
     if (path) wisdom_save_locked(path);
 }
@@ -391,7 +406,7 @@ static int count_candidates(const Plan &P, int pass) {
         const fast::VariantB *vb = P.dtype == GPUFFT_FLOAT ? fast::kVariantsB_f32 : fast::kVariantsB_f64;
         const int nb = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsB_f32 : fast::kNumVariantsB_f64;
         const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
-        for (int i = 0; i < nb; ++i) n += (vb[i].nx == nx && (vb[i].kind == 0 || rows16));
+        for (int i = 0; i < nb; ++i) n += (vb[i].nx == nx && (vb[i].kind != 1 || rows16));
     }
     return n;
 }
@@ -435,31 +450,45 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
     }
     cudaMemsetAsync(buf, 0, bytes, s);
     const int reps = bytes > (256u << 20) ? 3 : 10;
-    int best[2] = {-1, -1}, best_kdiv = 1;
+    int best[2] = {-1, -1}, best_k = 0;
     for (int pass = 0; pass < 2; ++pass) {
         const int n = count_candidates(*P, pass);
         float best_ms = 1e30f;
         for (int c = -1; c < n; ++c) {
-            // Pass A candidates are timed at the chosen cluster size, half and a quarter of it
-            for (int kdiv = 1; kdiv <= (pass == 0 && c >= 0 ? 4 : 1); kdiv *= 2) {
-                P->kdiv = pass == 0 ? kdiv : best_kdiv;
+            // Pass A candidates are timed at the cluster size chosen from the
+            // L2 size (K), at K/2 and K/4, at 16 when K is 8, and split into
+            // two launches
+            int ks[5] = {0, 0, 0, 0, 0}, nk = 1;
+            if (pass == 0 && c >= 0) {
+                P->kfix = 0;
+                setup_fast(*P, c, P->idx_b);
+                if (P->fa && P->fa->kind == 0) {
+                    const int k0 = P->k_fa;
+                    for (int k : {k0 / 2, k0 / 4, k0 == 8 ? 16 : 0})
+                        if (k >= 2) ks[nk++] = k;
+                    ks[nk++] = -1;
+                }
+            }
+            for (int ki = 0; ki < nk; ++ki) {
+                P->kfix = pass == 0 ? ks[ki] : best_k;
                 if (pass == 0)
                     setup_fast(*P, c, P->idx_b);
                 else
                     setup_fast(*P, best[0], c);
                 if ((pass == 0 && c >= 0 && !P->fa) || (pass == 1 && c >= 0 && !P->fb)) continue;
-                if (kdiv > 1 && (P->fa->kind != 0 || P->k_fa < 2)) continue;
+                if (pass == 0 && ks[ki] > 0 && P->k_fa != ks[ki]) continue;
+                if (pass == 0 && ks[ki] == -1 && !P->split_a) continue;
                 const float ms = time_pass(*P, buf, s, pass, reps);
                 if (ms < best_ms) {
                     best_ms = ms;
                     best[pass] = c;
-                    if (pass == 0) best_kdiv = kdiv;
+                    if (pass == 0) best_k = ks[ki];
                 }
             }
         }
     }
     if (!scratch) cudaFree(buf);
-    P->kdiv = best_kdiv;
+    P->kfix = best_k;
     const int rc = setup_fast(*P, best[0], best[1]);
     if (rc != GPUFFT_SUCCESS) return rc;
     P->tuned = true;
@@ -575,7 +604,7 @@ static int build_plan(Plan &P) {
         return GPUFFT_SUCCESS;
     }
     int ia = 0, ib = 0;
-    if (wisdom_lookup(P, ia, ib, P.kdiv)) P.tuned = true;
+    if (wisdom_lookup(P, ia, ib, P.kfix)) P.tuned = true;
     const char *va = std::getenv("GPUFFT_VARIANT_A"), *vb = std::getenv("GPUFFT_VARIANT_B");
     if (va) ia = std::atoi(va);
     if (vb) ib = std::atoi(vb);
@@ -628,8 +657,21 @@ template <typename T>
 static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
     PassAParams prm = P.pa;
     prm.data = data;
+    if (P.fa && P.split_a) {
+        // forward: z rows then y columns; inverse: y columns then z rows
+        prm.K = P.k_fa;
+        void *args[] = {&prm};
+        for (int half = 0; half < 2; ++half) {
+            prm.phases = (fwd == (half == 0)) ? 1 : 2;
+            const cudaError_t e = cudaLaunchKernel(fwd ? P.fa->kfwd : P.fa->kinv, dim3(P.grid_fa), dim3(P.fa->nt), args,
+                                                   P.fa->smem, s);
+            if (e != cudaSuccess) return cuda_error(e, "launch split pass A (specialised)");
+        }
+        return GPUFFT_SUCCESS;
+    }
     if (P.fa) {
         prm.K = P.k_fa;
+        prm.phases = 0;
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         cfg.gridDim = dim3(P.grid_fa, 1, 1);
@@ -727,7 +769,7 @@ static int plan_exec_pass_impl(const Plan *P, void *data, void *stream, int pass
     return pass == 0 ? launch_pass_a<double>(*P, data, s, forward) : launch_pass_b<double>(*P, data, s, forward);
 }
 
-int plan_launches(const Plan *P) { return P ? (P->nx == 1 ? 1 : 2) : 0; }
+int plan_launches(const Plan *P) { return P ? (P->nx == 1 ? 1 : 2) + (P->fa && P->split_a ? 1 : 0) : 0; }
 
 static void describe_axis(std::string &out, const char *name, const AxisPlan &ax) {
     char b[64];
@@ -759,8 +801,9 @@ int plan_describe(const Plan *P, char *buf, int len) {
              P->pb.wx, P->pb.ntiles);
     s += b;
     if (P->fa) {
-        snprintf(b, sizeof(b), " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu}", P->fa->kind, P->fa->ny, P->fa->m,
-                 P->fa->rw, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa, P->fa->smem);
+        snprintf(b, sizeof(b), " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu split=%d}",
+                 P->fa->kind, P->fa->ny, P->fa->m, P->fa->rw, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa,
+                 P->fa->smem, P->split_a ? 1 : 0);
         s += b;
     }
     if (P->fb) {

@@ -27,7 +27,9 @@ struct Plan {
     const fast::VariantB *fb = nullptr;
     int grid_fa = 0, grid_fb = 0, k_fa = 1, occ_fa = 0, occ_fb = 0;
     int idx_a = 0, idx_b = 0;  // registry candidate in use per pass (-1 = generic kernels)
-    int kdiv = 1;              // specialised Pass A cluster size = the chosen size / kdiv
+    int kfix = 0;              // specialised Pass A cluster size (0: chosen from the L2 size;
+                               // -1: split Pass A, z rows and y columns in two launches)
+    bool split_a = false;      // specialised Pass A runs as two launches (kfix == -1)
     bool tuned = false;
 };
 

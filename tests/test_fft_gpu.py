@@ -368,7 +368,8 @@ def test_autotune_keeps_results_identical_and_records_wisdom(oracle, cuda, tmp_p
 
 
 @pytest.mark.parametrize("grid,dt", [((512, 512, 512), "float"), ((512, 512, 512), "double"),
-                                     ((1024, 512, 256), "float"), ((256, 256, 256), "float")], ids=str)
+                                     ((1024, 512, 256), "float"), ((256, 256, 256), "float"),
+                                     ((16, 1024, 1024), "float")], ids=str)
 def test_every_compiled_candidate_matches_generic(cuda, grid, dt, monkeypatch):
     """The autotuner picks on speed alone, so every registered kernel candidate
     of both passes must compute the same transform as the generic kernels."""
@@ -405,3 +406,42 @@ def test_every_compiled_candidate_matches_generic(cuda, grid, dt, monkeypatch):
                 err = ((x - w).double().norm() / w.double().norm()).item()
                 assert err < tol, (tag, c, fwd, err, p.describe())
         monkeypatch.delenv(env)
+
+
+@pytest.mark.parametrize("k", [2, 4, 16, -1])
+def test_pass_a_cluster_size_does_not_change_results(cuda, tmp_path, k):
+    """The autotuner may run Pass A on clusters of 2..16 CTAs, or split into a
+    z-row launch and a y-column launch (k = -1), and keeps the choice in
+    wisdom files; every row and column is transformed the same way whichever
+    CTA or launch handles it, so the output is bitwise the default plan's."""
+    import torch
+    import gpu_fft_b200 as g
+
+    n = 512
+    gen = torch.Generator(device="cuda").manual_seed(21)
+    f = torch.zeros((n, n, n + 2), device="cuda")
+    f[:, :, :n] = torch.randn((n, n, n), generator=gen, device="cuda")
+    ref = f.clone()
+    base = g.Plan(n, n, n, "float")
+    base.r2c(ref)
+    path = tmp_path / "w.txt"
+    g.wisdom_save(str(path))
+    dev = torch.cuda.get_device_name(0).replace(" ", "_")
+    major, minor = torch.cuda.get_device_capability(0)
+    path.write_text(f"{dev}_sm{major * 10 + minor} 0 {n} {n} {n} 0 0 {k}\n")
+    g.wisdom_load(str(path))
+    p = g.Plan(n, n, n, "float")
+    assert (f"K={k} " if k > 0 else "split=1}") in p.describe(), p.describe()
+    assert p.launches() == (3 if k == -1 else 2)
+    out = f.clone()
+    p.r2c(out)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+    back = out.clone()
+    p.c2r(back)
+    base.c2r(out)
+    torch.cuda.synchronize()
+    assert torch.equal(back, out)
+    # leave the process-wide wisdom at the defaults for the tests that follow
+    path.write_text(f"{dev}_sm{major * 10 + minor} 0 {n} {n} {n} 0 0 0\n")
+    g.wisdom_load(str(path))
