@@ -34,7 +34,7 @@ EXPORTS = (
     "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
     "gpufft_batch_status", "gpufft_batch_items",
     "gpufft_plan16_create", "gpufft_plan16_destroy", "gpufft_plan16_scale_count", "gpufft_exec16_r2c",
-    "gpufft_exec16_c2r", "gpufft_quantize16", "gpufft_dequantize16",
+    "gpufft_exec16_c2r", "gpufft_exec16_pass", "gpufft_quantize16", "gpufft_dequantize16",
     "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
     "gpufft_server_submit", "gpufft_server_poll", "gpufft_server_wait", "gpufft_server_cancel", "gpufft_server_stats",
 )
@@ -104,6 +104,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_plan16_scale_count.restype = i64
     lib.gpufft_exec16_r2c.argtypes = [vp, vp, vp, vp]
     lib.gpufft_exec16_c2r.argtypes = [vp, vp, vp, vp]
+    lib.gpufft_exec16_pass.argtypes = [vp, vp, vp, vp, ci, ci]
     lib.gpufft_quantize16.argtypes = [vp, vp, vp, vp, vp]
     lib.gpufft_dequantize16.argtypes = [vp, vp, vp, vp, ci, vp]
     rp = ctypes.POINTER(Request)
@@ -331,6 +332,10 @@ class Plan16:
 
     def c2r_ptr(self, field: int, scales: int, stream: int = 0):
         _check(load_library().gpufft_exec16_c2r(self._h, field, scales, stream))
+
+    def pass_ptr(self, field: int, scales: int, stream: int, which: int, forward: bool) -> None:
+        """One kernel of the transform: which=0 Pass A (z,y), 1 Pass B (x)."""
+        _check(load_library().gpufft_exec16_pass(self._h, field, scales, stream, int(which), 1 if forward else 0))
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

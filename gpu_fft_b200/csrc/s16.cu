@@ -31,11 +31,12 @@ struct VarB {
      (const void *)pass_a_s16<FMT, NY, M, RW, WY, NT, true, 0, 0, MINB>,                                       \
      (const void *)pass_a_s16<FMT, NY, M, RW, WY, NT, false, 0, 0, MINB>}
 #define S16_B(FMT, NX, W, NT, MINB)                                                                             \
-    {FMT, NX, W, NT, 0, (size_t)(NX + NX * W) * sizeof(float2),                                                 \
+    {FMT, NX, W, NT, 0, (size_t)(NX + NX * W) * sizeof(float2) + (size_t)NX * W * sizeof(float),                \
      (const void *)pass_b_s16<FMT, NX, W, NT, true, 0, MINB>, (const void *)pass_b_s16<FMT, NX, W, NT, false, 0, MINB>}
 
 static const VarA kA[] = {
     S16_A(0, 1024, 512, 1, 8, 256, 2), S16_A(1, 1024, 512, 1, 8, 256, 2),
+    S16_A(0, 1024, 512, 1, 16, 512, 1), S16_A(1, 1024, 512, 1, 16, 512, 1),
     S16_A(0, 512, 256, 2, 8, 256, 2),  S16_A(1, 512, 256, 2, 8, 256, 2),
     S16_A(0, 384, 192, 1, 8, 256, 1),  S16_A(1, 384, 192, 1, 8, 256, 1),
     S16_A(0, 256, 128, 2, 8, 256, 2),  S16_A(1, 256, 128, 2, 8, 256, 2),
@@ -45,7 +46,8 @@ static const VarA kA[] = {
     S16_A(0, 64, 32, 4, 8, 256, 2),    S16_A(1, 64, 32, 4, 8, 256, 2),
 };
 static const VarB kB[] = {
-    S16_B(0, 1024, 8, 256, 2), S16_B(1, 1024, 8, 256, 2), S16_B(0, 512, 16, 256, 2), S16_B(1, 512, 16, 256, 2),
+    S16_B(0, 1024, 8, 256, 2), S16_B(1, 1024, 8, 256, 2),
+    S16_B(0, 1024, 16, 512, 1), S16_B(1, 1024, 16, 512, 1), S16_B(0, 512, 16, 256, 2), S16_B(1, 512, 16, 256, 2),
     S16_B(0, 256, 16, 256, 2), S16_B(1, 256, 16, 256, 2), S16_B(0, 128, 16, 256, 2), S16_B(1, 128, 16, 256, 2),
     S16_B(0, 64, 16, 256, 2),  S16_B(1, 64, 16, 256, 2),  S16_B(0, 384, 8, 256, 2),  S16_B(1, 384, 8, 256, 2),
     S16_B(0, 192, 16, 256, 2), S16_B(1, 192, 16, 256, 2), S16_B(0, 96, 16, 256, 2),  S16_B(1, 96, 16, 256, 2),
@@ -99,10 +101,13 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
     const int m = (int)(nz / 2);
     const VarA *va = nullptr;
     const VarB *vb = nullptr;
+    // first matching entry, or the i-th with GPUFFT_VARIANT16_A / _B (measurement)
+    const char *ea = std::getenv("GPUFFT_VARIANT16_A"), *eb = std::getenv("GPUFFT_VARIANT16_B");
+    int skip_a = ea ? std::max(0, std::atoi(ea)) : 0, skip_b = eb ? std::max(0, std::atoi(eb)) : 0;
     for (const auto &v : kA)
-        if (v.fmt == fmt && v.ny == ny && v.m == m) { va = &v; break; }
+        if (v.fmt == fmt && v.ny == ny && v.m == m && skip_a-- == 0) { va = &v; break; }
     for (const auto &v : kB)
-        if (v.fmt == fmt && v.nx == nx) { vb = &v; break; }
+        if (v.fmt == fmt && v.nx == nx && skip_b-- == 0) { vb = &v; break; }
     if (!va || !vb)
         return set_error(GPUFFT_ERR_UNSUPPORTED,
                          "16-bit storage form: grid %lldx%lldx%lld has no compiled kernels (cubic 64, 96, 128, "
@@ -293,6 +298,16 @@ extern "C" int64_t gpufft_plan16_scale_count(gpufft_plan16 plan) {
     const Plan16 *P = reinterpret_cast<const Plan16 *>(plan);
     if (!P) return -1;
     return std::max<int64_t>(P->nx * P->ny, P->ny * (P->nz / 2 + 1));
+}
+
+extern "C" int gpufft_exec16_pass(gpufft_plan16 plan, void *data, float *scales, void *stream, int pass, int forward) {
+    const Plan16 *P = reinterpret_cast<const Plan16 *>(plan);
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no 16-bit plan");
+    if (!data || !scales) return set_error(GPUFFT_ERR_INVALID, "data and scales must be device pointers");
+    if (((uintptr_t)data) % 4 || ((uintptr_t)scales) % 4) return set_error(GPUFFT_ERR_INVALID, "misaligned pointer");
+    if (pass != 0 && pass != 1) return set_error(GPUFFT_ERR_INVALID, "pass must be 0 (A) or 1 (B)");
+    return pass == 0 ? launch_a(*P, data, scales, (cudaStream_t)stream, forward != 0)
+                     : launch_b(*P, data, scales, (cudaStream_t)stream, forward != 0);
 }
 
 static int exec16(gpufft_plan16 plan, void *data, float *scales, void *stream, bool fwd) {

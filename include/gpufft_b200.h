@@ -161,7 +161,7 @@ int gpufft_batch_items(gpufft_batch batch);
  * (index x*Ny + y) before R2C / after C2R, per x-pencil scales of the
  * spectrum (index ky*(Nz/2+1) + kz) after R2C / before C2R.  A stored value
  * is value/scale with scale = max(|re|,|im|) over its pencil.  Grids with
- * compiled kernels: cubic powers of two from 64 to 1024.
+ * compiled kernels: cubic 64, 96, 128, 192, 256, 384, 512 and 1024.
  * ------------------------------------------------------------------------ */
 typedef struct gpufft_plan16_s *gpufft_plan16;
 int gpufft_plan16_create(gpufft_plan16 *plan, int64_t nx, int64_t ny, int64_t nz, int format);
@@ -169,6 +169,9 @@ int gpufft_plan16_destroy(gpufft_plan16 plan);
 int64_t gpufft_plan16_scale_count(gpufft_plan16 plan);
 int gpufft_exec16_r2c(gpufft_plan16 plan, void *data, float *scales, void *stream);
 int gpufft_exec16_c2r(gpufft_plan16 plan, void *data, float *scales, void *stream);
+/* One kernel of a 16-bit transform (pass 0 = A, 1 = B; forward 1 or 0), as
+ * gpufft_exec_pass: forward is A then B, inverse B then A. */
+int gpufft_exec16_pass(gpufft_plan16 plan, void *data, float *scales, void *stream, int pass, int forward);
 /* FP32 padded real field (Nx*Ny*2*(Nz/2+1) floats) -> 16-bit field + per-row scales. */
 int gpufft_quantize16(gpufft_plan16 plan, const float *field, void *data, float *row_scales, void *stream);
 /* 16-bit field -> FP32 (spectrum != 0: per x-pencil scales; else per z-row scales). */

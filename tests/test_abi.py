@@ -87,16 +87,16 @@ def test_argument_errors_are_reported_without_a_gpu(lib):
 
 def test_wisdom_file_round_trip(lib, tmp_path):
     """Wisdom files hold one line per (device, dtype, grid): the Pass A and
-    Pass B candidates and the Pass A cluster divisor (absent in older files,
-    read as 1).  Loading and saving them needs no GPU."""
+    Pass B candidates and the Pass A cluster size (absent in older files, read
+    as 0 = chosen from the L2 size).  Loading and saving them needs no GPU."""
     src = tmp_path / "w1.txt"
-    src.write_text("# comment\nNVIDIA_B200_sm100 0 512 512 512 0 1\nNVIDIA_B200_sm100 1 128 128 128 -1 0 2\n")
+    src.write_text("# comment\nNVIDIA_B200_sm100 0 512 512 512 0 1\nNVIDIA_B200_sm100 1 128 128 128 -1 0 4\n")
     assert lib.gpufft_wisdom_load(str(src).encode()) == 0
     dst = tmp_path / "w2.txt"
     assert lib.gpufft_wisdom_save(str(dst).encode()) == 0
     lines = [l for l in dst.read_text().splitlines() if not l.startswith("#")]
-    assert "NVIDIA_B200_sm100 0 512 512 512 0 1 1" in lines
-    assert "NVIDIA_B200_sm100 1 128 128 128 -1 0 2" in lines
+    assert "NVIDIA_B200_sm100 0 512 512 512 0 1 0" in lines
+    assert "NVIDIA_B200_sm100 1 128 128 128 -1 0 4" in lines
 
 
 def test_python_binding_errors(lib):
