@@ -37,6 +37,8 @@ EXPORTS = (
     "gpufft_exec16_c2r", "gpufft_exec16_pass", "gpufft_quantize16", "gpufft_dequantize16",
     "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
     "gpufft_server_submit", "gpufft_server_poll", "gpufft_server_wait", "gpufft_server_cancel", "gpufft_server_stats",
+    "gpufft_init_dist", "gpufft_dist_unique_id", "gpufft_dplan_create", "gpufft_dplan_destroy", "gpufft_dexec_r2c", "gpufft_dexec_c2r",
+    "gpufft_dplan_layout", "gpufft_dgroup_create", "gpufft_dgroup_exec",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 
@@ -117,6 +119,15 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_server_wait.argtypes = [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     lib.gpufft_server_cancel.argtypes = [vp, i64]
     lib.gpufft_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    lib.gpufft_dist_unique_id.argtypes = [vp]
+    lib.gpufft_init_dist.argtypes = [i64, i64, i64, ci, ci, ci, vp]
+    lib.gpufft_dplan_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci, ci, ci, vp]
+    lib.gpufft_dplan_destroy.argtypes = [vp]
+    lib.gpufft_dexec_r2c.argtypes = [vp, vp, vp]
+    lib.gpufft_dexec_c2r.argtypes = [vp, vp, vp]
+    lib.gpufft_dplan_layout.argtypes = [vp, ctypes.POINTER(i64)]
+    lib.gpufft_dgroup_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci, ci]
+    lib.gpufft_dgroup_exec.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ci, ci, vp]
     for name in EXPORTS:
         if getattr(lib, name, None) is None:
             raise ImportError(f"{path} does not export {name}")
@@ -349,6 +360,130 @@ class Plan16:
             pass
 
 
+# ---------------------------------------------------------------------------
+# slab decomposition over several GPUs (gpufft_dplan_* / gpufft_dgroup_*)
+# ---------------------------------------------------------------------------
+UNIQUE_ID_BYTES = 128
+
+
+def slab_layout(nx: int, ny: int, nz: int, procs: int, rank: int) -> dict:
+    """Rank `rank`'s share: real x-slab planes [x0, x0+nxl) as [nxl][Ny][2*Nh]
+    reals before R2C; spectral y-slab rows [y0, y0+nyl) as [Nx][nyl][Nh]
+    complex after it (the same buffer)."""
+    if nx % procs or ny % procs:
+        raise GpuFFTError(1, f"ERR_INVALID: Nx={nx} and Ny={ny} must be multiples of procs={procs}")
+    nxl, nyl, nh = nx // procs, ny // procs, nz // 2 + 1
+    return {"x0": rank * nxl, "nxl": nxl, "y0": rank * nyl, "nyl": nyl, "real_shape": (nxl, ny, 2 * nh),
+            "spectrum_shape": (nx, nyl, nh)}
+
+
+def dist_unique_id() -> bytes:
+    """Rank 0's NCCL unique id, to be handed to every rank."""
+    buf = ctypes.create_string_buffer(UNIQUE_ID_BYTES)
+    _check(load_library().gpufft_dist_unique_id(buf))
+    return buf.raw
+
+
+def broadcast_unique_id(group=None) -> bytes:
+    """Rank 0 of a torch.distributed group makes the NCCL unique id; every rank
+    returns it (broadcast over the group, any backend)."""
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.zeros(UNIQUE_ID_BYTES, dtype=torch.uint8, device=dev)
+    if dist.get_rank(group) == 0:
+        t.copy_(torch.frombuffer(bytearray(dist_unique_id()), dtype=torch.uint8))
+    dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
+    return bytes(t.cpu().tolist())
+
+
+class DistPlan:
+    """One rank of a slab-decomposed transform (gpufft_dplan_*): the
+    reference's INIT_GPU_FFT / GPU_FFT_R2C / GPU_FFT_C2R with procs > 1.  The
+    rank's device must be current; every rank creates its plan (a collective)
+    and runs the transforms in the same order."""
+
+    def __init__(self, nx: int, ny: int, nz: int, dtype="float", procs: int = 1, rank: int = 0,
+                 unique_id: bytes | None = None):
+        self.nx, self.ny, self.nz, self.procs, self.rank = int(nx), int(ny), int(nz), int(procs), int(rank)
+        self.dtype = _dtype_code(dtype)
+        idbuf = ctypes.create_string_buffer(unique_id, UNIQUE_ID_BYTES) if unique_id is not None else None
+        h = ctypes.c_void_p()
+        _check(load_library().gpufft_dplan_create(ctypes.byref(h), self.nx, self.ny, self.nz, self.dtype,
+                                                  self.procs, self.rank, idbuf))
+        self._h = h
+
+    @classmethod
+    def from_process_group(cls, nx, ny, nz, dtype="float", group=None):
+        """Create the plan on every rank of a torch.distributed group: rank 0's
+        unique id is broadcast over the group (any backend)."""
+        import torch
+        import torch.distributed as dist
+
+        procs, rank = dist.get_world_size(group), dist.get_rank(group)
+        uid = broadcast_unique_id(group) if procs > 1 else None
+        return cls(nx, ny, nz, dtype, procs, rank, uid)
+
+    def layout(self) -> dict:
+        out = (ctypes.c_int64 * 5)()
+        _check(load_library().gpufft_dplan_layout(self._h, out))
+        return {"x0": out[0], "nxl": out[1], "y0": out[2], "nyl": out[3], "elements": out[4]}
+
+    def r2c(self, field, stream=None) -> None:
+        _check(load_library().gpufft_dexec_r2c(self._h, field.data_ptr(), _stream_handle(stream)))
+
+    def c2r(self, field, stream=None) -> None:
+        _check(load_library().gpufft_dexec_c2r(self._h, field.data_ptr(), _stream_handle(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_dplan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DistGroup:
+    """All `procs` ranks of a slab decomposition in this process on the current
+    device, exchanging by device copies (gpufft_dgroup_*)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, dtype="float", procs: int = 2):
+        self.procs = int(procs)
+        self.dtype = _dtype_code(dtype)
+        self._h = (ctypes.c_void_p * self.procs)()
+        _check(load_library().gpufft_dgroup_create(self._h, int(nx), int(ny), int(nz), self.dtype, self.procs))
+
+    def _exec(self, fields, forward: bool, stream) -> None:
+        if len(fields) != self.procs:
+            raise GpuFFTError(1, f"ERR_INVALID: {len(fields)} fields for {self.procs} ranks")
+        ptrs = (ctypes.c_void_p * self.procs)(*[f.data_ptr() for f in fields])
+        _check(load_library().gpufft_dgroup_exec(self._h, ptrs, self.procs, 1 if forward else 0, _stream_handle(stream)))
+
+    def r2c(self, fields, stream=None) -> None:
+        self._exec(fields, True, stream)
+
+    def c2r(self, fields, stream=None) -> None:
+        self._exec(fields, False, stream)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            for i in range(self.procs):
+                if self._h[i]:
+                    load_library().gpufft_dplan_destroy(ctypes.c_void_p(self._h[i]))
+                    self._h[i] = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 PRECISIONS = {"f32": 0, "float": 0, "f64": 1, "double": 1, "bf16": 2, "fp16": 3}
 REQ_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -418,9 +553,22 @@ class Server:
 # ---------------------------------------------------------------------------
 # reference-shaped API (GPU_FFT::INIT_GPU_FFT / GPU_FFT_R2C / GPU_FFT_C2R)
 # ---------------------------------------------------------------------------
-def INIT_GPU_FFT(nx: int, ny: int, nz: int, procs: int = 1, rank: int = 0, dtype="float") -> None:
-    """GPU_FFT::INIT_GPU_FFT<T1,T2>(Nx,Ny,Nz,procs,rank,comm) (GPU_FFT_init.cu:41-93)."""
-    _check(load_library().gpufft_init(int(nx), int(ny), int(nz), _dtype_code(dtype), int(procs), int(rank)))
+def INIT_GPU_FFT(nx: int, ny: int, nz: int, procs: int = 1, rank: int = 0, dtype="float", comm=None) -> None:
+    """GPU_FFT::INIT_GPU_FFT<T1,T2>(Nx,Ny,Nz,procs,rank,comm) (GPU_FFT_init.cu:41-93).
+    With procs > 1 every rank calls it (a collective); `comm` is a
+    torch.distributed group (None = the default group) over which rank 0's
+    NCCL unique id is broadcast, and the process-wide plan becomes the
+    slab-decomposed one (x-slab in, y-slab out)."""
+    if int(procs) == 1:
+        _check(load_library().gpufft_init(int(nx), int(ny), int(nz), _dtype_code(dtype), 1, int(rank)))
+        return
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        raise GpuFFTError(1, f"ERR_INVALID: procs={procs} needs an initialised torch.distributed group to share "
+                             "rank 0's NCCL unique id")
+    uid = ctypes.create_string_buffer(broadcast_unique_id(comm), UNIQUE_ID_BYTES)
+    _check(load_library().gpufft_init_dist(int(nx), int(ny), int(nz), _dtype_code(dtype), int(procs), int(rank), uid))
 
 
 def _field_dtype(field) -> int:

@@ -827,12 +827,15 @@ using namespace gpufft;
 
 namespace {
 std::mutex g_mu;
-Plan *g_global[2] = {nullptr, nullptr};  // the reference-shaped singleton, one per dtype
+// the reference-shaped process-wide plan, one per dtype: single-GPU or slab-decomposed
+Plan *g_global[2] = {nullptr, nullptr};
+DistPlan *g_dist[2] = {nullptr, nullptr};
 }  // namespace
 
 extern "C" int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank) {
     if (procs != 1 || rank != 0)
-        return set_error(GPUFFT_ERR_UNSUPPORTED, "procs=%d rank=%d: only a size-1 communicator is supported", procs,
+        return set_error(GPUFFT_ERR_UNSUPPORTED,
+                         "procs=%d rank=%d: more than one rank needs the NCCL unique id (gpufft_init_dist)", procs,
                          rank);
     Plan *P = nullptr;
     const int rc = plan_create(&P, nx, ny, nz, dtype, 0);
@@ -840,6 +843,21 @@ extern "C" int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int pr
     std::lock_guard<std::mutex> lk(g_mu);
     plan_destroy(g_global[dtype]);
     g_global[dtype] = P;
+    dist_free(g_dist[dtype]);
+    g_dist[dtype] = nullptr;
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_init_dist(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank, const void *id) {
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return set_error(GPUFFT_ERR_INVALID, "bad dtype %d", dtype);
+    gpufft_dplan D = nullptr;
+    const int rc = gpufft_dplan_create(&D, nx, ny, nz, dtype, procs, rank, id);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    std::lock_guard<std::mutex> lk(g_mu);
+    dist_free(g_dist[dtype]);
+    g_dist[dtype] = reinterpret_cast<DistPlan *>(D);
+    plan_destroy(g_global[dtype]);
+    g_global[dtype] = nullptr;
     return GPUFFT_SUCCESS;
 }
 
@@ -849,8 +867,14 @@ static Plan *global_plan(int dtype) {
     return g_global[dtype];
 }
 
+static DistPlan *global_dist(int dtype) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_dist[dtype];
+}
+
 extern "C" int gpufft_r2c(int dtype, void *data, void *stream) {
     if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return set_error(GPUFFT_ERR_INVALID, "bad dtype %d", dtype);
+    if (DistPlan *D = global_dist(dtype)) return dist_exec(D, data, (cudaStream_t)stream, true);
     Plan *P = global_plan(dtype);
     if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "gpufft_r2c: no %s plan; call gpufft_init first",
                              dtype == GPUFFT_FLOAT ? "float" : "double");
@@ -859,6 +883,7 @@ extern "C" int gpufft_r2c(int dtype, void *data, void *stream) {
 
 extern "C" int gpufft_c2r(int dtype, void *data, void *stream) {
     if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE) return set_error(GPUFFT_ERR_INVALID, "bad dtype %d", dtype);
+    if (DistPlan *D = global_dist(dtype)) return dist_exec(D, data, (cudaStream_t)stream, false);
     Plan *P = global_plan(dtype);
     if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "gpufft_c2r: no %s plan; call gpufft_init first",
                              dtype == GPUFFT_FLOAT ? "float" : "double");
@@ -870,6 +895,10 @@ extern "C" int gpufft_finalize(void) {
     for (auto &p : g_global) {
         plan_destroy(p);
         p = nullptr;
+    }
+    for (auto &d : g_dist) {
+        dist_free(d);
+        d = nullptr;
     }
     return GPUFFT_SUCCESS;
 }

@@ -39,6 +39,10 @@ const char *last_error();
 // least `bytes`.  Never lowers it: plans of different sizes share the generic
 // kernels, and a later, smaller plan must not undo an earlier plan's limit.
 cudaError_t raise_smem_limit(const void *fn, size_t bytes);
+// slab-decomposed plans (dist.cu), for the reference-shaped process-wide plans
+struct DistPlan;
+int dist_exec(DistPlan *D, void *data, cudaStream_t s, bool fwd);
+void dist_free(DistPlan *D);
 int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
 int plan_destroy(Plan *P);
 int plan_exec(const Plan *P, void *data, void *stream, bool forward);

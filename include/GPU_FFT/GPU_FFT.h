@@ -23,7 +23,9 @@
  *    (FFT_definations.cu:45-77); these templates keep void signatures and
  *    print gpufft_last_error() to stderr, and abort if the environment
  *    variable GPUFFT_ABORT_ON_ERROR is set to a non-empty value other than 0;
- *  - procs must be 1 (rank 0): the multi-GPU slab exchange is not provided;
+ *  - with procs > 1 (real MPI) the exchange is NCCL, set up from rank 0's
+ *    unique id broadcast over the communicator; the slab layouts are the
+ *    reference's (x-slab in, y-slab out);
  *  - float and double plans coexist (the reference's INIT never switches
  *    its cuFFT types back to float, GPU_FFT_init.cu:77-83);
  *  - gpufft_finalize() frees the plans (the reference leaks them).
@@ -148,8 +150,8 @@ inline int comm_size(MPI_Comm &comm, int fallback) {
 template <typename T1, typename T2>
 inline void INIT_GPU_FFT_COMM(int procs, int rank, MPI_Comm &MPI_COMMUNICATOR_INPUT) {
     const int size = detail::comm_size(MPI_COMMUNICATOR_INPUT, procs);
-    if (procs != 1 || rank != 0 || size != 1)
-        detail::report(GPUFFT_ERR_UNSUPPORTED, "INIT_GPU_FFT_COMM (only a size-1 communicator is supported)");
+    if (procs != size || rank < 0 || rank >= size)
+        detail::report(GPUFFT_ERR_INVALID, "INIT_GPU_FFT_COMM (procs and rank must match the communicator)");
 }
 
 template <typename T1, typename T2>
@@ -158,8 +160,23 @@ inline void INIT_GPU_FFT(int64 Nx_in, int64 Ny_in, int64 Nz_in, int procs, int r
     static_assert(std::is_same<T1, TRANSITIONS::T1_f>::value || std::is_same<T1, TRANSITIONS::T1_d>::value,
                   "T1,T2 must be float,cufftComplex or double,cufftDoubleComplex");
     const int size = detail::comm_size(MPI_COMMUNICATOR_INPUT, procs);
-    const int p = (size != procs) ? size : procs;
-    detail::report(gpufft_init(Nx_in, Ny_in, Nz_in, detail::dtype_of<T1, T2>::value, p, rank), "INIT_GPU_FFT");
+    const int p = (size != procs) ? size : procs;  // the communicator decides
+    if (p == 1) {
+        detail::report(gpufft_init(Nx_in, Ny_in, Nz_in, detail::dtype_of<T1, T2>::value, 1, rank), "INIT_GPU_FFT");
+        return;
+    }
+    // more ranks: rank 0's NCCL unique id is broadcast over the communicator,
+    // then every rank joins the slab-decomposed plan (a collective)
+    unsigned char id[GPUFFT_UNIQUE_ID_BYTES] = {0};
+    int rc = rank == 0 ? gpufft_dist_unique_id(id) : GPUFFT_SUCCESS;
+    MPI_Bcast(&rc, 1, MPI_INT, 0, MPI_COMMUNICATOR_INPUT);
+    if (rc != GPUFFT_SUCCESS) {
+        detail::report(rc, "INIT_GPU_FFT (NCCL unique id)");
+        return;
+    }
+    MPI_Bcast(id, GPUFFT_UNIQUE_ID_BYTES, MPI_BYTE, 0, MPI_COMMUNICATOR_INPUT);
+    detail::report(gpufft_init_dist(Nx_in, Ny_in, Nz_in, detail::dtype_of<T1, T2>::value, p, rank, id),
+                   "INIT_GPU_FFT");
 }
 
 template <typename T1, typename T2>

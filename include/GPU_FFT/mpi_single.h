@@ -21,6 +21,8 @@ typedef struct {
 #define MPI_COMM_SELF ((MPI_Comm)1)
 #define MPI_C_COMPLEX ((MPI_Datatype)1)
 #define MPI_C_DOUBLE_COMPLEX ((MPI_Datatype)2)
+#define MPI_BYTE ((MPI_Datatype)3)
+#define MPI_INT ((MPI_Datatype)4)
 #define MPI_STATUS_IGNORE ((MPI_Status *)0)
 #define MPI_STATUSES_IGNORE ((MPI_Status *)0)
 #define MPI_SUCCESS 0
@@ -37,6 +39,7 @@ inline int MPI_Comm_size(MPI_Comm, int *size) {
     return MPI_SUCCESS;
 }
 inline int MPI_Barrier(MPI_Comm) { return MPI_SUCCESS; }
+inline int MPI_Bcast(void *, int, MPI_Datatype, int root, MPI_Comm) { return root == 0 ? MPI_SUCCESS : MPI_ERR_RANK; }
 inline int MPI_Isend(const void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request *) { return MPI_ERR_RANK; }
 inline int MPI_Irecv(void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request *) { return MPI_ERR_RANK; }
 inline int MPI_Waitall(int count, MPI_Request *, MPI_Status *) { return count == 0 ? MPI_SUCCESS : MPI_ERR_RANK; }

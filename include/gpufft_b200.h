@@ -55,10 +55,19 @@ typedef struct gpufft_plan_s *gpufft_plan;
  * (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT_init.cu:41-93, with
  * INIT_GPU_FFT_COMM, communications_setup.cu:56-71).  Builds (or rebuilds) the
  * process-wide plan of `dtype` on the current CUDA device.  procs must be 1
- * (rank 0); procs > 1 returns GPUFFT_ERR_UNSUPPORTED.  Unlike the reference,
- * float and double plans coexist, re-initialising frees the previous plan,
- * and no field-sized scratch buffer is allocated. */
+ * (rank 0) here; more ranks go through gpufft_init_dist.  Unlike the
+ * reference, float and double plans coexist, re-initialising frees the
+ * previous plan, and no field-sized scratch buffer is allocated. */
 int gpufft_init(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank);
+
+/* The same with procs > 1 ranks, one GPU each (the reference's MPI case,
+ * GPU_FFT_init.cu:41-93 and communications_setup.cu:56-71): a collective of
+ * all ranks, given rank 0's NCCL unique id (gpufft_dist_unique_id, below).
+ * gpufft_r2c / gpufft_c2r then run the slab-decomposed transform: x-slab
+ * [Nx/p][Ny][2(Nz/2+1)] in, y-slab [Nx][Ny/p][Nz/2+1] out (FFT_R2C.cu:41-70).
+ * Needs one exchange buffer of the local slab's size (the reference
+ * allocates one of the field's size, GPU_FFT_init.cu:50). */
+int gpufft_init_dist(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank, const void *id);
 
 /* Replaces GPU_FFT::GPU_FFT_R2C<T1,T2>(T1*) (FFT_implementation/FFT_R2C.cu:41-70):
  * in-place forward transform of `data` on `stream`. */
@@ -177,6 +186,37 @@ int gpufft_quantize16(gpufft_plan16 plan, const float *field, void *data, float 
 /* 16-bit field -> FP32 (spectrum != 0: per x-pencil scales; else per z-row scales). */
 int gpufft_dequantize16(gpufft_plan16 plan, const void *data, const float *scales, float *out, int spectrum,
                         void *stream);
+
+/* --------------------------------------------------------------------------
+ * Slab decomposition over `procs` GPUs, one process (rank) each — the
+ * reference's procs > 1 path: INIT_GPU_FFT with procs/rank/comm
+ * (GPU_FFT_init.cu:41-93, communications_setup.cu:56-71) and GPU_FFT_R2C /
+ * GPU_FFT_C2R (FFT_R2C.cu:41-70, FFT_C2R.cu:41-70).  Rank r's buffer holds
+ * the real x-slab [Nx/p][Ny][2(Nz/2+1)] (planes r*Nx/p ...) before R2C and the
+ * spectral y-slab [Nx][Ny/p][Nz/2+1] (ky = r*Ny/p ...) after it, in place; Nx
+ * and Ny must be multiples of procs.  The exchange is NCCL (loaded at run
+ * time): rank 0 calls gpufft_dist_unique_id, hands the 128 bytes to every rank
+ * (MPI_Bcast, torch.distributed, ...), and every rank calls
+ * gpufft_dplan_create with its device current (a collective; bounded by
+ * GPUFFT_DIST_INIT_TIMEOUT seconds, default 120).  procs = 1 needs no id (given
+ * one, the exchange runs through a one-rank NCCL communicator all the same).
+ * ------------------------------------------------------------------------ */
+typedef struct gpufft_dplan_s *gpufft_dplan;
+#define GPUFFT_UNIQUE_ID_BYTES 128
+int gpufft_dist_unique_id(void *id);
+int gpufft_dplan_create(gpufft_dplan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank,
+                        const void *id);
+int gpufft_dplan_destroy(gpufft_dplan plan);
+/* Every rank calls these in the same order (each issues one all-to-all). */
+int gpufft_dexec_r2c(gpufft_dplan plan, void *data, void *stream);
+int gpufft_dexec_c2r(gpufft_dplan plan, void *data, void *stream);
+/* out[5]: first x-plane and x-planes of the real slab, first ky and ky rows of
+ * the spectral slab, complex elements of the local buffer. */
+int gpufft_dplan_layout(gpufft_dplan plan, int64_t *out);
+/* All `procs` ranks in this process on the current device, exchanging by
+ * device copies (no NCCL): the same decomposition on one GPU. */
+int gpufft_dgroup_create(gpufft_dplan *plans, int64_t nx, int64_t ny, int64_t nz, int dtype, int procs);
+int gpufft_dgroup_exec(gpufft_dplan *plans, void **data, int procs, int forward, void *stream);
 
 /* --------------------------------------------------------------------------
  * Serving: a continuous-batching request loop (no counterpart in the

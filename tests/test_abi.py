@@ -62,7 +62,7 @@ def test_field_bytes(lib):
 def test_argument_errors_are_reported_without_a_gpu(lib):
     # procs > 1: the multi-GPU slab path is not provided
     assert lib.gpufft_init(8, 8, 8, 0, 2, 0) == 2
-    assert b"size-1" in lib.gpufft_last_error()
+    assert b"gpufft_init_dist" in lib.gpufft_last_error()
     assert lib.gpufft_init(8, 8, 8, 0, 1, 1) == 2
     # bad sizes, bad dtype, odd Nz
     assert lib.gpufft_init(0, 8, 8, 0, 1, 0) == 1
@@ -103,8 +103,8 @@ def test_python_binding_errors(lib):
     import gpu_fft_b200 as g
 
     with pytest.raises(g.GpuFFTError) as e:
-        g.INIT_GPU_FFT(8, 8, 8, procs=4, rank=0)
-    assert e.value.code == 2
+        g.INIT_GPU_FFT(8, 8, 8, procs=4, rank=0)  # no process group to share the NCCL id over
+    assert e.value.code == 1
     with pytest.raises(ValueError):
         g.INIT_GPU_FFT(8, 8, 8, dtype="int8")
     assert g.field_shape(512, 512, 512) == (512, 512, 514)
