@@ -175,13 +175,27 @@ struct TileFFT {
             }
         }
         if (dst_smem) sync();  // every reader of the tile is done before it is overwritten
+        // In the COLS layout a thread's butterflies are NT/W apart in i; when
+        // that is a multiple of p they share k = i mod p, so their twiddles
+        // are read from shared memory once.
+        constexpr bool shared_k = LAYOUT == COLS && p > 1 && C > 1 && (NT / W) % p == 0 && NT % W == 0;
+        V tws[shared_k ? R : 1];
+        if constexpr (shared_k) {
+            constexpr int off = stage_offset(F, S);
+            const int k0 = ii[0] % p;
+#pragma unroll
+            for (int j = 1; j < R; ++j) tws[j] = tw[off + (j - 1) * p + k0];
+        }
 #pragma unroll
         for (int m = 0; m < C; ++m) {
             const int q = tid + m * NT;
             if (items % NT == 0 || q < items) {
                 const int i = ii[m], w = ww[m];
                 const int k = i % p;
-                if constexpr (p > 1) {
+                if constexpr (shared_k) {
+#pragma unroll
+                    for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tws[j]);
+                } else if constexpr (p > 1) {
                     constexpr int off = stage_offset(F, S);
 #pragma unroll
                     for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tw[off + (j - 1) * p + k]);
