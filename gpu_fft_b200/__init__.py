@@ -28,7 +28,7 @@ STATUS = {0: "SUCCESS", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4
 EXPORTS = (
     "gpufft_init", "gpufft_r2c", "gpufft_c2r", "gpufft_finalize", "gpufft_last_error",
     "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_exec_r2c", "gpufft_exec_c2r",
-    "gpufft_exec_pass", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
+    "gpufft_exec_pass", "gpufft_exec_r2c_ex", "gpufft_exec_c2r_ex", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
     "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
     "gpufft_exec_noalloc",
     "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
@@ -85,6 +85,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_exec_r2c.argtypes = [vp, vp, vp]
     lib.gpufft_exec_c2r.argtypes = [vp, vp, vp]
     lib.gpufft_exec_pass.argtypes = [vp, vp, vp, ci, ci]
+    lib.gpufft_exec_r2c_ex.argtypes = [vp, vp, vp, ctypes.c_double, ci]
+    lib.gpufft_exec_c2r_ex.argtypes = [vp, vp, vp, ctypes.c_double]
     lib.gpufft_field_bytes.argtypes = [i64, i64, i64, ci]
     lib.gpufft_field_bytes.restype = i64
     lib.gpufft_plan_launches.argtypes = [vp]
@@ -206,11 +208,21 @@ class Plan:
             raise ValueError(f"field holds {field.numel() * field.element_size()} bytes, the grid needs {need}")
         return field.data_ptr()
 
-    def r2c(self, field, stream=None):
+    def r2c(self, field, stream=None, scale: float = 1.0, dealias: bool = False):
+        """In-place R2C; `scale` multiplies the spectrum and `dealias` zeroes
+        the modes outside the 2/3-rule box, both fused into the x pass."""
+        if scale != 1.0 or dealias:
+            _check(load_library().gpufft_exec_r2c_ex(self._h, self._ptr(field), _stream_handle(stream), float(scale),
+                                                     1 if dealias else 0))
+            return
         _check(load_library().gpufft_exec_r2c(self._h, self._ptr(field), _stream_handle(stream)))
         return field
 
-    def c2r(self, field, stream=None):
+    def c2r(self, field, stream=None, scale: float = 1.0):
+        """In-place C2R; `scale` (e.g. 1/(Nx*Ny*Nz)) is fused into the x pass."""
+        if scale != 1.0:
+            _check(load_library().gpufft_exec_c2r_ex(self._h, self._ptr(field), _stream_handle(stream), float(scale)))
+            return
         _check(load_library().gpufft_exec_c2r(self._h, self._ptr(field), _stream_handle(stream)))
         return field
 

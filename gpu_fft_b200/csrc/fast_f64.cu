@@ -17,10 +17,14 @@ namespace fast {
      (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, false, VY, VZ, MINB>}
 #define P_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
     {1, DT, NX, W, NT, V, (size_t)(((NX + 1) / 2 * 2) + 2 * NX * W) * sizeof(cx_t<T>),                          \
-     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB>}
+     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB>,  \
+     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB, true>,                                                  \
+     (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB, true>}
 #define B_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
     {0, DT, NX, W, NT, V, (size_t)(NX + NX * W) * sizeof(cx_t<T>), (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB>, \
-     (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB>}
+     (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB>,                                                       \
+     (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB, true>,                                                  \
+     (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB, true>}
 
 const VariantA kVariantsA_f64[] = {
     A_ENTRY(double, 1, 512, 256, 2, 8, 256, 0, 0, 2),

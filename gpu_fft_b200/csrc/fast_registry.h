@@ -29,6 +29,7 @@ struct VariantB {
     int w, nt, v;
     size_t smem;
     const void *kfwd, *kinv;
+    const void *kfwd_epi, *kinv_epi;  // the same with the x-pass epilogue (scale, dealiasing)
 };
 
 // all entries of one precision (defined in fast_f32.cu / fast_f64.cu)

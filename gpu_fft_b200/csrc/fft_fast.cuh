@@ -256,7 +256,8 @@ struct TileFFT {
 // ---------------------------------------------------------------------------
 // Pass B: x-axis FFT over column tiles (stride Ny*Nh), compile-time Nx
 // ---------------------------------------------------------------------------
-template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB>
+// EPI: the x-pass epilogue (scale, dealiasing; PassBParams) is compiled in
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB, bool EPI = false>
 __global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
     using V = cx_t<T>;
     using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
@@ -275,7 +276,12 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
             return (w < wv) ? ld_g(g + (long long)n * ncols + w) : V{(T)0, (T)0};
         };
         auto dst = [&](int n, int w, V v) {
-            if (w < wv) st_g(g + (long long)n * ncols + w, v);
+            if (w < wv) {
+                if constexpr (EPI)
+                    st_g(g + (long long)n * ncols + w, pass_b_epilogue(P, v, n, c0 + w));
+                else
+                    st_g(g + (long long)n * ncols + w, v);
+            }
         };
         FFT::run(src, dst, tile, tw);
     }
@@ -298,7 +304,7 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB>
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB, bool EPI = false>
 __global__ void __launch_bounds__(NT, MINB) pass_b_pipe(PassBParams P) {
     using V = cx_t<T>;
     using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
@@ -344,7 +350,12 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_pipe(PassBParams P) {
         const int wv = (int)min((long long)W, ncols - c0);
         V *g = obase + c0;
         auto dst = [&](int n, int w, V v) {
-            if (w < wv) st_g(g + (long long)n * ncols + w, v);
+            if (w < wv) {
+                if constexpr (EPI)
+                    st_g(g + (long long)n * ncols + w, pass_b_epilogue(P, v, n, c0 + w));
+                else
+                    st_g(g + (long long)n * ncols + w, v);
+            }
         };
         FromSmem fs;
         FFT::run(fs, dst, cur, tw);

@@ -85,7 +85,29 @@ struct PassBParams {
     FastDiv wxdiv;
     AxisPlan ax;
     long long ntiles;
+    // Epilogue fused into the x pass (the last pass of R2C, the first of
+    // C2R), on when epi != 0: every stored value times `scale`; with
+    // `dealias` (R2C) modes outside the 2/3-rule box |kx| <= Nx/3,
+    // |ky| <= Ny/3, kz <= Nz/3 are stored as zero.  ny, nh, nz decode a
+    // column c = ky*Nh + kz.
+    int epi, dealias;
+    double scale;
+    int ny, nh, nz;
 };
+
+// the x pass's store of value v at (kx, column), with the epilogue applied
+template <typename V>
+__device__ __forceinline__ V pass_b_epilogue(const PassBParams &P, V v, int kx, long long col) {
+    using T = decltype(v.x);
+    if (P.dealias) {
+        const int c = (int)col;  // Ny*Nh < 2^31 (checked at plan time)
+        const int ky = c / P.nh, kz = c - ky * P.nh;
+        const int fx = min(kx, P.nx - kx), fy = min(ky, P.ny - ky);
+        if (3 * fx > P.nx || 3 * fy > P.ny || 3 * kz > P.nz) return V{(T)0, (T)0};
+    }
+    const T s = (T)P.scale;
+    return V{v.x * s, v.y * s};
+}
 
 // ---------------------------------------------------------------------------
 // global memory access: L2-only loads (the plane written in phase 1 is read
@@ -399,7 +421,15 @@ __global__ void __launch_bounds__(kThreads) pass_b_kernel(PassBParams P) {
         load_cols<T>(ta, base + c0, P.ncols, P.nx, P.wx, P.wxdiv, wv);
         __syncthreads();
         V *res = fft_tile<T, FWD>(ta, tb, P.wx, 1, P.wx, P.wxdiv, P.ax, twx);
-        store_cols<T>(res, base + c0, P.ncols, P.nx, P.wx, P.wxdiv, 0, wv);
+        if (P.epi) {
+            for (int q = threadIdx.x; q < P.nx * P.wx; q += kThreads) {
+                const int r = (int)fdiv((uint32_t)q, P.wxdiv);
+                const int w = q - r * P.wx;
+                if (w < wv) st_g(base + c0 + (long long)r * P.ncols + w, pass_b_epilogue(P, res[q], r, c0 + w));
+            }
+        } else {
+            store_cols<T>(res, base + c0, P.ncols, P.nx, P.wx, P.wxdiv, 0, wv);
+        }
         __syncthreads();
     }
 }

@@ -285,7 +285,7 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         }
     }
     if (P.fb) {
-        for (const void *k : {P.fb->kfwd, P.fb->kinv}) {
+        for (const void *k : {P.fb->kfwd, P.fb->kinv, P.fb->kfwd_epi, P.fb->kinv_epi}) {
             cudaError_t e = raise_smem_limit(k, P.fb->smem);
             if (e != cudaSuccess) {
                 cudaGetLastError();
@@ -556,6 +556,12 @@ static int build_plan(Plan &P) {
     B.nx = nx; B.ncols = (long long)ny * nh; B.wx = wx; B.wxdiv = make_fastdiv(wx);
     fill_axis(B.ax, nx, rx, 1);
     B.ntiles = (B.ncols + wx - 1) / wx;
+    B.epi = 0;
+    B.dealias = 0;
+    B.scale = 1.0;
+    B.ny = ny;
+    B.nh = nh;
+    B.nz = nz;
     P.smem_b = (size_t)(nx + 2 * (size_t)nx * wx) * vs;
 
     // ---- twiddle tables on the device
@@ -706,16 +712,19 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
 }
 
 template <typename T>
-static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd) {
+static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd, double scale = 1.0, int dealias = 0) {
     if (P.nx == 1) return GPUFFT_SUCCESS;  // a length-1 DFT is the identity
     PassBParams prm = P.pb;
     prm.data = data;
+    prm.scale = scale;
+    prm.dealias = dealias;
+    prm.epi = (scale != 1.0 || dealias) ? 1 : 0;
     if (P.fb && !(P.fb->kind == 1 && ((uintptr_t)data) % 16 != 0)) {
         prm.wx = P.fb->w;
         prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
         void *args[] = {&prm};
-        const cudaError_t e = cudaLaunchKernel(fwd ? P.fb->kfwd : P.fb->kinv, dim3(P.grid_fb), dim3(P.fb->nt), args,
-                                               P.fb->smem, s);
+        const void *k = prm.epi ? (fwd ? P.fb->kfwd_epi : P.fb->kinv_epi) : (fwd ? P.fb->kfwd : P.fb->kinv);
+        const cudaError_t e = cudaLaunchKernel(k, dim3(P.grid_fb), dim3(P.fb->nt), args, P.fb->smem, s);
         return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass B (specialised)");
     }
     if (fwd)
@@ -726,31 +735,38 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd) {
     return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass B");
 }
 
-int plan_exec(const Plan *P, void *data, void *stream, bool forward) {
+int plan_exec_ex(const Plan *P, void *data, void *stream, bool forward, double scale, int dealias) {
     if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
     if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
     if (((uintptr_t)data) % (P->dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
         return set_error(GPUFFT_ERR_INVALID, "data pointer is not aligned to its complex type");
+    if ((scale != 1.0 || dealias) && P->nx == 1)
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "Nx = 1 has no x pass to fuse the scale or dealiasing into");
+    if (dealias && !forward) return set_error(GPUFFT_ERR_INVALID, "dealiasing is fused into R2C only");
     cudaStream_t s = (cudaStream_t)stream;
     int rc;
     if (P->dtype == GPUFFT_FLOAT) {
         if (forward) {
             rc = launch_pass_a<float>(*P, data, s, true);
-            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<float>(*P, data, s, true);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<float>(*P, data, s, true, scale, dealias);
         } else {
-            rc = launch_pass_b<float>(*P, data, s, false);
+            rc = launch_pass_b<float>(*P, data, s, false, scale);
             if (rc == GPUFFT_SUCCESS) rc = launch_pass_a<float>(*P, data, s, false);
         }
     } else {
         if (forward) {
             rc = launch_pass_a<double>(*P, data, s, true);
-            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<double>(*P, data, s, true);
+            if (rc == GPUFFT_SUCCESS) rc = launch_pass_b<double>(*P, data, s, true, scale, dealias);
         } else {
-            rc = launch_pass_b<double>(*P, data, s, false);
+            rc = launch_pass_b<double>(*P, data, s, false, scale);
             if (rc == GPUFFT_SUCCESS) rc = launch_pass_a<double>(*P, data, s, false);
         }
     }
     return rc;
+}
+
+int plan_exec(const Plan *P, void *data, void *stream, bool forward) {
+    return plan_exec_ex(P, data, stream, forward, 1.0, 0);
 }
 
 int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward) {
@@ -938,6 +954,14 @@ extern "C" int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream) {
 
 extern "C" int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream) {
     return plan_exec(reinterpret_cast<Plan *>(plan), data, stream, false);
+}
+
+extern "C" int gpufft_exec_r2c_ex(gpufft_plan plan, void *data, void *stream, double scale, int dealias) {
+    return plan_exec_ex(reinterpret_cast<Plan *>(plan), data, stream, true, scale, dealias);
+}
+
+extern "C" int gpufft_exec_c2r_ex(gpufft_plan plan, void *data, void *stream, double scale) {
+    return plan_exec_ex(reinterpret_cast<Plan *>(plan), data, stream, false, scale, 0);
 }
 
 extern "C" int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int forward) {

@@ -46,6 +46,7 @@ void dist_free(DistPlan *D);
 int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
 int plan_destroy(Plan *P);
 int plan_exec(const Plan *P, void *data, void *stream, bool forward);
+int plan_exec_ex(const Plan *P, void *data, void *stream, bool forward, double scale, int dealias);
 int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward);
 int plan_launches(const Plan *P);
 int plan_describe(const Plan *P, char *buf, int len);

@@ -93,6 +93,15 @@ int gpufft_plan_create(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, in
 int gpufft_plan_destroy(gpufft_plan plan);
 int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream);
 int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream);
+/* The same with an epilogue fused into the x pass, for pseudo-spectral steps
+ * (the reference leaves normalisation to the caller's own kernel,
+ * GPU_FFT_TEST_SCRIPT/test.cu:53-65): every output value is multiplied by
+ * `scale` (1.0 = none; 1/(Nx*Ny*Nz) makes C2R the normalised inverse), and
+ * with dealias != 0 R2C stores zero for the modes outside the 2/3-rule box
+ * |kx| <= Nx/3, |ky| <= Ny/3, kz <= Nz/3.  No extra pass over the field;
+ * Nx must be at least 2. */
+int gpufft_exec_r2c_ex(gpufft_plan plan, void *data, void *stream, double scale, int dealias);
+int gpufft_exec_c2r_ex(gpufft_plan plan, void *data, void *stream, double scale);
 
 /* One of the two kernels of an exec, for per-kernel timing and for callers
  * that fuse their own work between the passes.  pass 0 = Pass A (z and y
