@@ -256,19 +256,21 @@ struct TileFFT {
 // ---------------------------------------------------------------------------
 // Pass B: x-axis FFT over column tiles (stride Ny*Nh), compile-time Nx
 // ---------------------------------------------------------------------------
-// EPI: the x-pass epilogue (scale, dealiasing; PassBParams) is compiled in
-template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB, bool EPI = false>
-__global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
+// Tiles first_tile, first_tile + tile_step, ... of Pass B (the kernel below
+// runs it over the grid; the batched form runs single tiles).  EPI: the
+// x-pass epilogue (scale, dealiasing; PassBParams) is compiled in.
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, bool EPI>
+__device__ __forceinline__ void pass_b_fast_run(const PassBParams &P, unsigned char *smem_raw, long long first_tile,
+                                                long long tile_step) {
     using V = cx_t<T>;
     using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tw = reinterpret_cast<V *>(smem_raw);
     V *tile = tw + NX;
     for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
     // (the first stage's barrier orders these writes before any twiddle read)
     V *base = reinterpret_cast<V *>(P.data);
     const long long ncols = P.ncols;
-    for (long long t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+    for (long long t = first_tile; t < P.ntiles; t += tile_step) {
         const long long c0 = t * W;
         const int wv = (int)min((long long)W, ncols - c0);
         V *g = base + c0;
@@ -285,6 +287,12 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
         };
         FFT::run(src, dst, tile, tw);
     }
+}
+
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB, bool EPI = false>
+__global__ void __launch_bounds__(NT, MINB) pass_b_fast(PassBParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pass_b_fast_run<T, NX, W, NT, FWD, VARIANT, EPI>(P, smem_raw, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -389,8 +397,13 @@ __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
-template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB>
-__global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
+// One CTA's part of Pass A: CTA `crank` of the K that share each x-plane
+// (rows [crank*NY/K, ...), column tiles crank, crank+K, ...), for planes
+// first_plane, first_plane + plane_step, ...  The kernel below runs it over
+// the grid; the batched form runs it for one whole plane (K = 1).
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ>
+__device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned char *smem_raw, const int crank,
+                                                const int K, const int first_plane, const int plane_step) {
     using V = cx_t<T>;
     using Shape = PassAShape<T, NY, M, RW, WY, NT, VY, VZ>;
     using RowFFT = TileFFT<T, M, RW, 32, FWD, ROWS, VZ, WARP>;
@@ -400,7 +413,6 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     constexpr int NH = M + 1;
     constexpr int UNP = Shape::UNP;
     constexpr int HALF = M / 2 + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     V *unp = reinterpret_cast<V *>(smem_raw);
     V *stz = unp + UNP;
     V *sty = stz + M;
@@ -410,10 +422,7 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     for (int q = threadIdx.x; q < NY - 1; q += NT) sty[q] = reinterpret_cast<const V *>(P.sty)[q];
     __syncthreads();
 
-    const int K = P.K;
-    const int crank = blockIdx.x % K;
-    const int cid = blockIdx.x / K;
-    const int ncl = gridDim.x / K;
+    const int cid = first_plane, ncl = plane_step;
     const int rows_per = (NY + K - 1) / K;
     const int rb = min(NY, crank * rows_per), re = min(NY, rb + rows_per);
     constexpr int ntiles_y = (M + WY - 1) / WY;
@@ -584,6 +593,14 @@ __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
         }
         __syncthreads();
     }
+}
+
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = P.K;
+    pass_a_fast_run<T, NY, M, RW, WY, NT, FWD, VY, VZ>(P, smem_raw, (int)blockIdx.x % K, K, (int)blockIdx.x / K,
+                                                       (int)gridDim.x / K);
 }
 
 // ---------------------------------------------------------------------------
