@@ -1,30 +1,10 @@
 // fast_f32.cu — FP32 instantiations of the compile-time specialised passes.
 // Tile shapes: column tiles of 8 or 16 complex (64/128-byte rows), row tiles
 // of whole rows per warp, 256 threads per CTA; see fft_fast.cuh.
-#include "fast_registry.h"
-#include "fft_fast.cuh"
+#include "fast_entries.h"
 
 namespace gpufft {
 namespace fast {
-
-#define A_ENTRY(T, DT, NY, M, RW, WY, NT, VY, VZ, MINB)                                                      \
-    {0, 0, DT, NY, M, RW, WY, NT, VY, VZ, PassAShape<T, NY, M, RW, WY, NT, VY, VZ>::smem_bytes(),              \
-     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, true, VY, VZ, MINB>,                                     \
-     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, false, VY, VZ, MINB>}
-#define D_ENTRY(T, DT, NY, M, RW, WY, NT, K, VY, VZ, MINB)                                                   \
-    {1, K, DT, NY, M, RW, WY, NT, VY, VZ, PassADsmemShape<T, NY, M, RW, WY, NT, K, VY, VZ>::smem_bytes(),        \
-     (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, true, VY, VZ, MINB>,                                    \
-     (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, false, VY, VZ, MINB>}
-#define P_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
-    {1, DT, NX, W, NT, V, (size_t)(((NX + 1) / 2 * 2) + 2 * NX * W) * sizeof(cx_t<T>),                          \
-     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB>,  \
-     (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB, true>,                                                  \
-     (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB, true>}
-#define B_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
-    {0, DT, NX, W, NT, V, (size_t)(NX + NX * W) * sizeof(cx_t<T>), (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB>, \
-     (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB>,                                                       \
-     (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB, true>,                                                  \
-     (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB, true>}
 
 const VariantA kVariantsA_f32[] = {
     A_ENTRY(float, 0, 512, 256, 2, 8, 256, 0, 0, 3),

@@ -37,6 +37,10 @@ extern const VariantA kVariantsA_f32[];
 extern const int kNumVariantsA_f32;
 extern const VariantB kVariantsB_f32[];
 extern const int kNumVariantsB_f32;
+extern const VariantA kVariantsA_f32s[];  // 3-smooth lengths (fast_f32_3s.cu)
+extern const int kNumVariantsA_f32s;
+extern const VariantB kVariantsB_f32s[];
+extern const int kNumVariantsB_f32s;
 extern const VariantA kVariantsA_f64[];
 extern const int kNumVariantsA_f64;
 extern const VariantB kVariantsB_f64[];

@@ -25,7 +25,8 @@ namespace fast {
 
 // ---------------------------------------------------------------------------
 // compile-time radix lists (same rule as the host factorize(): the power of
-// two split into balanced stages of at most 16, then odd primes 3..13).
+// two split into balanced stages of at most 16, then pairs of 3s as radix 9,
+// then odd primes 3..13).
 // VARIANT 1 prefers radix-16 stages for the power-of-two part.
 // ---------------------------------------------------------------------------
 struct Fac {
@@ -52,6 +53,11 @@ __host__ __device__ constexpr Fac factor(int N, int variant) {
             const int k = (a + 3) / 4;
             for (int s = 0; s < k; ++s) f.r[f.n++] = 1 << (a / k + (s < a % k ? 1 : 0));
         }
+    }
+    // pairs of 3s as radix-9 stages (3x3 in registers): fewer passes over the tile
+    while (m % 9 == 0) {
+        f.r[f.n++] = 9;
+        m /= 9;
     }
     const int primes[5] = {3, 5, 7, 11, 13};
     for (int pi = 0; pi < 5; ++pi)

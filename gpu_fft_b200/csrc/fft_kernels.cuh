@@ -171,6 +171,7 @@ __device__ __forceinline__ cx_t<T> *fft_tile(cx_t<T> *a, cx_t<T> *b, int sn, int
             case 5: stage<T, 5, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
             case 7: stage<T, 7, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
             case 8: stage<T, 8, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
+            case 9: stage<T, 9, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
             case 11: stage<T, 11, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
             case 13: stage<T, 13, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;
             case 16: stage<T, 16, FWD>(a, b, sn, sw, W, wdiv, ax.n, p, pd, tws, tw); break;

@@ -3,8 +3,8 @@
 // Every length-R DFT here computes y[k] = sum_j x[j] * exp(s*2*pi*i*j*k/R)
 // with s = -1 (FWD) or +1 (inverse), unscaled — the convention of the
 // transforms GPU_FFT calls (cuFFT FORWARD/INVERSE, FFT_R2C.cu:69, FFT_C2R.cu:45).
-// Radix 2, 4, 8 and 16 are hand-factored (4 = 2x2, 8 = 2x4, 16 = 4x4 with
-// constant twiddles); odd primes 3..13 use the symmetric pair form
+// Radix 2, 4, 8, 9 and 16 are hand-factored (4 = 2x2, 8 = 2x4, 9 = 3x3,
+// 16 = 4x4 with constant twiddles); odd primes 3..13 use the symmetric pair form
 //   y[k] = x0 + sum_{j<=(R-1)/2} cos(2pi jk/R)(x_j + x_{R-j})  -/+  i sin(2pi jk/R)(x_j - x_{R-j}).
 // The trigonometric constants are the mathematical values written out to
 // 25 significant digits and rounded by the compiler to the storage type.
@@ -118,6 +118,23 @@ template <> struct Trig<13> {
     }
 };
 
+// cos/sin(2*pi*m/9), m = 0..8 (twiddles inside the radix-9 DFT)
+struct Trig9 {
+    static __host__ __device__ constexpr double c(int i) {
+        constexpr double t[9] = {1.0, 0.7660444431189780352023927, 0.1736481776669303488517166, -0.5,
+                                 -0.9396926207859083840541093, -0.9396926207859083840541093, -0.5,
+                                 0.1736481776669303488517166, 0.7660444431189780352023927};
+        return t[i];
+    }
+    static __host__ __device__ constexpr double s(int i) {
+        constexpr double t[9] = {0.0, 0.6427876096865393263226434, 0.984807753012208059366743,
+                                 0.8660254037844386467637232, 0.3420201433256687330440996,
+                                 -0.3420201433256687330440996, -0.8660254037844386467637232,
+                                 -0.984807753012208059366743, -0.6427876096865393263226434};
+        return t[i];
+    }
+};
+
 // cos/sin(2*pi*m/16), m = 0..15
 struct Trig16 {
     static __host__ __device__ constexpr double c(int i) {
@@ -170,6 +187,31 @@ template <bool FWD, typename V> __device__ __forceinline__ void dft4(V &x0, V &x
     x2 = c_sub(t0, t2);
     x1 = c_add(t1, t3);
     x3 = c_sub(t1, t3);
+}
+
+// length-3 DFT in place: y0 = a+b+c, y1,2 = a - (b+c)/2 -/+ i (sqrt3/2)(b-c) (forward)
+template <bool FWD, typename V> __device__ __forceinline__ void dft3(V &a, V &b, V &c) {
+    using T = decltype(a.x);
+    const T h = (T)0.5, s3 = (T)0.8660254037844386467637232;
+    const V sp = c_add(b, c), sm = c_sub(b, c);
+    const V m = V{a.x - h * sp.x, a.y - h * sp.y};
+    const V r = V{s3 * sm.x, s3 * sm.y};  // multiplied by -i (forward) or +i below
+    a = c_add(a, sp);
+    const V ir = c_rot<FWD>(r);
+    b = c_add(m, ir);
+    c = c_sub(m, ir);
+}
+
+// x * exp(s*2*pi*i*m/9) for compile-time m (s = -1 forward, +1 inverse)
+template <bool FWD, int M, typename V> __device__ __forceinline__ V tw9(V a) {
+    using T = decltype(a.x);
+    constexpr int m = M % 9;
+    if constexpr (m == 0) return a;
+    else {
+        const T c = (T)Trig9::c(m);
+        const T s = FWD ? -(T)Trig9::s(m) : (T)Trig9::s(m);
+        return V{a.x * c - a.y * s, a.x * s + a.y * c};
+    }
 }
 
 template <int R, bool FWD, typename V> struct Dft;
@@ -226,6 +268,29 @@ template <bool FWD, typename V> struct Dft<16, FWD, V> {
         t = x[6]; x[6] = x[9]; x[9] = t;
         t = x[7]; x[7] = x[13]; x[13] = t;
         t = x[11]; x[11] = x[14]; x[14] = t;
+    }
+};
+
+// radix 9 = 3 x 3: DFT3 over x[j + 3m] for j = 0..2, twiddle w9^(j*k1),
+// DFT3 over j, then the 3x3 index transpose (as radix 16 = 4 x 4)
+template <bool FWD, typename V> struct Dft<9, FWD, V> {
+    static __device__ __forceinline__ void run(V *x) {
+        dft3<FWD>(x[0], x[3], x[6]);
+        dft3<FWD>(x[1], x[4], x[7]);
+        dft3<FWD>(x[2], x[5], x[8]);
+        // F_j[k1] sits at x[j + 3*k1]
+        x[4] = tw9<FWD, 1>(x[4]);
+        x[7] = tw9<FWD, 2>(x[7]);
+        x[5] = tw9<FWD, 2>(x[5]);
+        x[8] = tw9<FWD, 4>(x[8]);
+        dft3<FWD>(x[0], x[1], x[2]);
+        dft3<FWD>(x[3], x[4], x[5]);
+        dft3<FWD>(x[6], x[7], x[8]);
+        // y[k1 + 3*k2] is at x[3*k1 + k2]: transpose the 3x3 index
+        V t;
+        t = x[1]; x[1] = x[3]; x[3] = t;
+        t = x[2]; x[2] = x[6]; x[6] = t;
+        t = x[5]; x[5] = x[7]; x[7] = t;
     }
 };
 

@@ -69,7 +69,7 @@ static int cuda_error(cudaError_t e, const char *what) {
 // ---------------------------------------------------------------------------
 // Radix list for a length-n FFT: the power-of-two part split into as few
 // stages of at most 16 as possible with balanced sizes (512 -> 8,8,8;
-// 1024 -> 16,8,8), then the odd prime factors 3, 5, 7, 11, 13.
+// 1024 -> 16,8,8), then pairs of 3s as 9s, then the odd primes 3, 5, 7, 11, 13.
 bool factorize(int n, std::vector<int> &radices) {
     radices.clear();
     if (n < 1) return false;
@@ -82,6 +82,7 @@ bool factorize(int n, std::vector<int> &radices) {
             radices.push_back(1 << bits);
         }
     }
+    while (r % 9 == 0) { radices.push_back(9); r /= 9; }  // pairs of 3s: radix-9 stages
     for (int p : {3, 5, 7, 11, 13})
         while (r % p == 0) { radices.push_back(p); r /= p; }
     return r == 1;
@@ -215,14 +216,36 @@ static int max_clusters(const void *kernel, int K, int nx, size_t smem, int nt, 
     return n;
 }
 
+// Every specialisation of a precision, in a fixed order (the main table,
+// then the table of 3-smooth lengths); candidate indices refer to it.
+static const std::vector<fast::VariantA> &variants_a(int dtype) {
+    static const std::vector<fast::VariantA> f32 = [] {
+        std::vector<fast::VariantA> v(fast::kVariantsA_f32, fast::kVariantsA_f32 + fast::kNumVariantsA_f32);
+        v.insert(v.end(), fast::kVariantsA_f32s, fast::kVariantsA_f32s + fast::kNumVariantsA_f32s);
+        return v;
+    }();
+    static const std::vector<fast::VariantA> f64(fast::kVariantsA_f64, fast::kVariantsA_f64 + fast::kNumVariantsA_f64);
+    return dtype == GPUFFT_FLOAT ? f32 : f64;
+}
+
+static const std::vector<fast::VariantB> &variants_b(int dtype) {
+    static const std::vector<fast::VariantB> f32 = [] {
+        std::vector<fast::VariantB> v(fast::kVariantsB_f32, fast::kVariantsB_f32 + fast::kNumVariantsB_f32);
+        v.insert(v.end(), fast::kVariantsB_f32s, fast::kVariantsB_f32s + fast::kNumVariantsB_f32s);
+        return v;
+    }();
+    static const std::vector<fast::VariantB> f64(fast::kVariantsB_f64, fast::kVariantsB_f64 + fast::kNumVariantsB_f64);
+    return dtype == GPUFFT_FLOAT ? f32 : f64;
+}
+
 // Picks the specialised kernels for this plan's shape (first registry entry,
 // or the entries named by the autotuner) and sizes their launches.
 static int setup_fast(Plan &P, int idx_a, int idx_b) {
     const int vs = P.dtype == GPUFFT_FLOAT ? 8 : 16;
-    const fast::VariantA *va = P.dtype == GPUFFT_FLOAT ? fast::kVariantsA_f32 : fast::kVariantsA_f64;
-    const int na = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsA_f32 : fast::kNumVariantsA_f64;
-    const fast::VariantB *vb = P.dtype == GPUFFT_FLOAT ? fast::kVariantsB_f32 : fast::kVariantsB_f64;
-    const int nb = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsB_f32 : fast::kNumVariantsB_f64;
+    const fast::VariantA *va = variants_a(P.dtype).data();
+    const int na = (int)variants_a(P.dtype).size();
+    const fast::VariantB *vb = variants_b(P.dtype).data();
+    const int nb = (int)variants_b(P.dtype).size();
     const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
     const int sms = device_sms(P.device);
     P.fa = nullptr;
@@ -399,12 +422,12 @@ static int count_candidates(const Plan &P, int pass) {
     const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
     int n = 0;
     if (pass == 0) {
-        const fast::VariantA *va = P.dtype == GPUFFT_FLOAT ? fast::kVariantsA_f32 : fast::kVariantsA_f64;
-        const int na = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsA_f32 : fast::kNumVariantsA_f64;
+        const fast::VariantA *va = variants_a(P.dtype).data();
+        const int na = (int)variants_a(P.dtype).size();
         for (int i = 0; i < na; ++i) n += (va[i].ny == ny && va[i].m == m);
     } else {
-        const fast::VariantB *vb = P.dtype == GPUFFT_FLOAT ? fast::kVariantsB_f32 : fast::kVariantsB_f64;
-        const int nb = P.dtype == GPUFFT_FLOAT ? fast::kNumVariantsB_f32 : fast::kNumVariantsB_f64;
+        const fast::VariantB *vb = variants_b(P.dtype).data();
+        const int nb = (int)variants_b(P.dtype).size();
         const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
         for (int i = 0; i < nb; ++i) n += (vb[i].nx == nx && (vb[i].kind != 1 || rows16));
     }
