@@ -35,6 +35,9 @@ using fast::TileLayout;
 using fast::ToSmem;
 using fast::WARP;
 using fast::BLOCK;
+using fast::cp_async16;
+using fast::cp_async_commit;
+using fast::cp_async_wait;
 
 // storage formats: 0 = bf16, 1 = fp16; a complex (or a pair of reals) is 32 bits
 template <int FMT> struct Fmt;
@@ -172,6 +175,139 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_s16(PassB16Params P) {
             const int n = q / W, w = q % W;
             if (w < wv) F::store(g + (long long)n * ncols + w, mulf(tile[L::idx(n, w)], inv_of(__uint_as_float(cmax[w]))));
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pass B, 16-bit storage, tiles double-buffered by cp.async.  While a tile is
+// transformed, the next one's 16-bit values (and, forward, its per-(x, kz)
+// input scales) stream into the other buffers.  The last FFT stage keeps its
+// values in registers: each thread's values all belong to one column, so the
+// column max is a register max, one shuffle and a shared-memory atomic, and
+// the scaled 16-bit values are stored straight from registers — no extra
+// passes over the tile.  Requires NT % W == 0, rows of the 16-bit field
+// 16-byte aligned (Ny*Nh a multiple of 4) and W a multiple of 4.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <int NX, int W>
+struct PassB16PipeShape {
+    // stage tables | 2 x 16-bit tiles | 2 x input scales (forward) | FP32 tile
+    static constexpr size_t raw_bytes = (size_t)NX * W * 4;
+    static constexpr size_t smem_bytes() {
+        return (size_t)NX * 8 + 2 * raw_bytes + 2 * (size_t)NX * W * 4 + (size_t)NX * W * 8;
+    }
+};
+
+template <int FMT, int NX, int W, int NT, bool FWD, int VARIANT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pass_b_s16_pipe(PassB16Params P) {
+    using V = float2;
+    using F = Fmt<FMT>;
+    using FFT = TileFFT<float, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
+    static_assert(NT % W == 0 && W % 4 == 0, "a thread's values share one column; 16-byte row chunks");
+    static_assert(((NX / FFT::F.r[FFT::NS - 1]) * W) % NT == 0, "every thread holds the same number of outputs");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    uint32_t *raw0 = reinterpret_cast<uint32_t *>(tw + NX);
+    uint32_t *raw1 = raw0 + NX * W;
+    float *sc0 = reinterpret_cast<float *>(raw1 + NX * W);
+    float *sc1 = sc0 + NX * W;
+    V *tile = reinterpret_cast<V *>(sc1 + NX * W);
+    __shared__ unsigned cmax[W];
+    __shared__ float colsc[W];
+    for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = P.stw[q];
+    const long long ncols = P.ncols;
+    const int nh = P.nh;
+    const int w_me = (int)threadIdx.x % W;  // the column of every value this thread holds
+    auto prefetch = [&](long long t, uint32_t *raw, float *sc) {
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        for (int q = threadIdx.x; q < NX * (W / 4); q += NT) {
+            const int n = q / (W / 4), ch = q % (W / 4);
+            const int valid = max(0, min(4, wv - ch * 4));
+            const uint32_t *src = P.data + (long long)n * ncols + c0 + (valid > 0 ? ch * 4 : 0);
+            cp_async16(raw + n * W + ch * 4, src, valid * 4);
+        }
+        if (FWD) {
+            const int kz0 = (int)(c0 % nh);
+            for (int q = threadIdx.x; q < NX * W; q += NT) {
+                const int n = q / W, w = q % W;
+                if (w < wv) {
+                    int kz = kz0 + w;
+                    if (kz >= nh) kz %= nh;
+                    cp_async4(sc + q, P.ms + (long long)n * nh + kz);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    long long t = blockIdx.x;
+    if (t < P.ntiles) prefetch(t, raw0, sc0);
+    int k = 0;
+    for (; t < P.ntiles; t += gridDim.x, k ^= 1) {
+        uint32_t *raw = k ? raw1 : raw0;
+        float *sc = k ? sc1 : sc0;
+        const long long tn = t + gridDim.x;
+        if (tn < P.ntiles) {
+            prefetch(tn, k ? raw0 : raw1, k ? sc0 : sc1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        if (threadIdx.x < W) {
+            cmax[threadIdx.x] = 0u;
+            if (!FWD) colsc[threadIdx.x] = (int)threadIdx.x < wv ? __ldg(&P.ks[c0 + threadIdx.x]) : 0.f;
+        }
+        __syncthreads();  // the tile's copies (every thread's), cmax and colsc are in place
+        auto src = [&](int n, int w) -> V {
+            if (w >= wv) return V{0.f, 0.f};
+            const int q = n * W + w;
+            uint32_t u = raw[q];
+            float2 v;
+            if constexpr (FMT == 0) {
+                __nv_bfloat162 h;
+                memcpy(&h, &u, 4);
+                v = __bfloat1622float2(h);
+            } else {
+                __half2 h;
+                memcpy(&h, &u, 4);
+                v = __half22float2(h);
+            }
+            return mulf(v, FWD ? sc[q] : colsc[w]);
+        };
+        // the last stage's values go to registers, in call order
+        constexpr int NOUT = NX * W / NT;
+        V out[NOUT];
+        int orow[NOUT];
+        int slot = 0;
+        auto dst = [&](int n, int w, V v) {
+            out[slot] = v;
+            orow[slot] = n;
+            ++slot;
+        };
+        FFT::run(src, dst, tile, tw);
+        float m = 0.f;
+#pragma unroll
+        for (int i = 0; i < NOUT; ++i) m = fmaxf(m, amax(out[i]));
+        // lanes w, w+W, w+2W, ... of a warp hold the same column
+#pragma unroll
+        for (int o = W; o < 32; o <<= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) < W) atomicMax(&cmax[w_me], __float_as_uint(m));
+        __syncthreads();
+        const float cm = __uint_as_float(cmax[w_me]);
+        const float inv = inv_of(cm);
+        if (w_me < wv) {
+            uint32_t *g = P.data + c0 + w_me;
+#pragma unroll
+            for (int i = 0; i < NOUT; ++i) F::store(g + (long long)orow[i] * ncols, mulf(out[i], inv));
+            if ((int)threadIdx.x < W) (FWD ? P.ks : P.ms2)[c0 + w_me] = cm;
+        }
+        __syncthreads();  // buffers, cmax and colsc are free for the next tile
     }
 }
 

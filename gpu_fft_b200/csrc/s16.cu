@@ -24,6 +24,7 @@ struct VarB {
     int fmt, nx, w, nt, v;
     size_t smem;
     const void *kfwd, *kinv;
+    int pipe = 0;  // 1: cp.async double-buffered (needs 16-byte aligned rows and data)
 };
 
 #define S16_A(FMT, NY, M, RW, WY, NT, MINB)                                                                     \
@@ -45,7 +46,13 @@ static const VarA kA[] = {
     S16_A(0, 96, 48, 2, 8, 256, 2),    S16_A(1, 96, 48, 2, 8, 256, 2),
     S16_A(0, 64, 32, 4, 8, 256, 2),    S16_A(1, 64, 32, 4, 8, 256, 2),
 };
+#define S16_P(FMT, NX, W, NT, MINB)                                                                             \
+    {FMT, NX, W, NT, 0, PassB16PipeShape<NX, W>::smem_bytes(), (const void *)pass_b_s16_pipe<FMT, NX, W, NT, true, 0, MINB>, \
+     (const void *)pass_b_s16_pipe<FMT, NX, W, NT, false, 0, MINB>, 1}
+
 static const VarB kB[] = {
+    S16_P(0, 512, 16, 256, 1), S16_P(1, 512, 16, 256, 1), S16_P(0, 256, 16, 256, 1), S16_P(1, 256, 16, 256, 1),
+    S16_P(0, 1024, 8, 256, 1), S16_P(1, 1024, 8, 256, 1),
     S16_B(0, 1024, 8, 256, 2), S16_B(1, 1024, 8, 256, 2),
     S16_B(0, 1024, 16, 512, 1), S16_B(1, 1024, 16, 512, 1), S16_B(0, 512, 16, 256, 2), S16_B(1, 512, 16, 256, 2),
     S16_B(0, 256, 16, 256, 2), S16_B(1, 256, 16, 256, 2), S16_B(0, 128, 16, 256, 2), S16_B(1, 128, 16, 256, 2),
@@ -59,10 +66,11 @@ struct Plan16 {
     int device = 0;
     const VarA *va = nullptr;
     const VarB *vb = nullptr;
+    const VarB *vb_plain = nullptr;  // for data that is not 16-byte aligned when vb is a pipelined entry
     void *tables = nullptr;  // twz | stz | sty | stw (float2)
     float *ms = nullptr, *ms2 = nullptr;
     const float2 *twz = nullptr, *stz = nullptr, *sty = nullptr, *stw = nullptr;
-    int K = 1, grid_a = 0, grid_b = 0;
+    int K = 1, grid_a = 0, grid_b = 0, grid_b_plain = 0;
 };
 
 static std::vector<float> stage_table_f32(int n) {
@@ -106,15 +114,21 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
     int skip_a = ea ? std::max(0, std::atoi(ea)) : 0, skip_b = eb ? std::max(0, std::atoi(eb)) : 0;
     for (const auto &v : kA)
         if (v.fmt == fmt && v.ny == ny && v.m == m && skip_a-- == 0) { va = &v; break; }
+    const int64_t nh16 = nz / 2 + 1;
+    const bool rows16 = (ny * nh16) % 4 == 0;  // 16-bit rows start on 16-byte boundaries
     for (const auto &v : kB)
-        if (v.fmt == fmt && v.nx == nx && skip_b-- == 0) { vb = &v; break; }
+        if (v.fmt == fmt && v.nx == nx && (!v.pipe || rows16) && skip_b-- == 0) { vb = &v; break; }
+    const VarB *vb_plain = nullptr;
+    for (const auto &v : kB)
+        if (v.fmt == fmt && v.nx == nx && !v.pipe) { vb_plain = &v; break; }
+    if (vb && !vb_plain) vb = nullptr;
     if (!va || !vb)
         return set_error(GPUFFT_ERR_UNSUPPORTED,
                          "16-bit storage form: grid %lldx%lldx%lld has no compiled kernels (cubic 64, 96, 128, "
                          "192, 256, 384, 512 and 1024 are built)", (long long)nx, (long long)ny, (long long)nz);
     Plan16 *P = new (std::nothrow) Plan16();
     if (!P) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
-    P->nx = nx; P->ny = ny; P->nz = nz; P->fmt = fmt; P->va = va; P->vb = vb;
+    P->nx = nx; P->ny = ny; P->nz = nz; P->fmt = fmt; P->va = va; P->vb = vb; P->vb_plain = vb_plain;
     cudaGetDevice(&P->device);
     // tables: w_Nz (unpack roots), stage tables of Nz/2, Ny and Nx
     std::vector<float> t;
@@ -149,8 +163,9 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
     P->stw = tb + ox;
     for (const void *k : {va->kfwd, va->kinv})
         if (e == cudaSuccess) e = raise_smem_limit(k, va->smem);
-    for (const void *k : {vb->kfwd, vb->kinv})
-        if (e == cudaSuccess) e = raise_smem_limit(k, vb->smem);
+    for (const VarB *b : {vb, vb_plain})
+        for (const void *k : {b->kfwd, b->kinv})
+            if (e == cudaSuccess) e = raise_smem_limit(k, b->smem);
     if (e != cudaSuccess) {
         plan16_free(P);
         return set_error(GPUFFT_ERR_CUDA, "16-bit plan set-up: %s", cudaGetErrorString(e));
@@ -192,6 +207,9 @@ static int plan16_create(Plan16 **out, int64_t nx, int64_t ny, int64_t nz, int f
     }
     const long long tiles = (ny * nh + vb->w - 1) / vb->w;
     P->grid_b = (int)std::min<long long>(tiles, (long long)occb * sms);
+    int occp = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occp, vb_plain->kfwd, vb_plain->nt, vb_plain->smem);
+    P->grid_b_plain = (int)std::min<long long>((ny * nh + vb_plain->w - 1) / vb_plain->w, (long long)std::max(occp, 1) * sms);
     *out = P;
     return GPUFFT_SUCCESS;
 }
@@ -233,10 +251,13 @@ static int launch_b(const Plan16 &P, void *data, float *scales, cudaStream_t s, 
     prm.stw = P.stw;
     prm.nh = (int)(P.nz / 2 + 1);
     prm.ncols = P.ny * prm.nh;
-    prm.ntiles = (prm.ncols + P.vb->w - 1) / P.vb->w;
+    // a pipelined entry copies 16-byte chunks: unaligned data takes the plain kernel
+    const bool plain = P.vb->pipe && ((uintptr_t)data % 16 != 0);
+    const VarB &b = plain ? *P.vb_plain : *P.vb;
+    prm.ntiles = (prm.ncols + b.w - 1) / b.w;
     void *args[] = {&prm};
     const cudaError_t e =
-        cudaLaunchKernel(fwd ? P.vb->kfwd : P.vb->kinv, dim3(P.grid_b), dim3(P.vb->nt), args, P.vb->smem, s);
+        cudaLaunchKernel(fwd ? b.kfwd : b.kinv, dim3(plain ? P.grid_b_plain : P.grid_b), dim3(b.nt), args, b.smem, s);
     return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "16-bit pass B: %s", cudaGetErrorString(e));
 }
 
