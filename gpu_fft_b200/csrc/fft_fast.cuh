@@ -160,7 +160,7 @@ struct TileFFT {
 #pragma unroll
         for (int m = 0; m < C; ++m) {
             const int q = tid + m * NT;
-            if (items % NT == 0 || q < items) {
+            if ((m + 1) * NT <= items || q < items) {
                 int i, w;
                 if constexpr (LAYOUT == COLS) {
                     w = q % W;
@@ -195,7 +195,7 @@ struct TileFFT {
 #pragma unroll
         for (int m = 0; m < C; ++m) {
             const int q = tid + m * NT;
-            if (items % NT == 0 || q < items) {
+            if ((m + 1) * NT <= items || q < items) {
                 const int i = ii[m], w = ww[m];
                 const int k = i % p;
                 if constexpr (shared_k) {
