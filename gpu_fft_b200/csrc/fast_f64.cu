@@ -9,6 +9,11 @@ namespace fast {
 const VariantA kVariantsA_f64[] = {
     A_ENTRY(double, 1, 512, 256, 2, 8, 256, 0, 0, 2),
     A_ENTRY(double, 1, 512, 256, 2, 4, 256, 0, 0, 2),
+    // 1024x512x256: planes of 512 x 129
+    A_ENTRY(double, 1, 512, 128, 2, 8, 256, 0, 0, 1),
+    A_ENTRY(double, 1, 512, 128, 2, 4, 256, 0, 0, 1),
+    // 128^3 (the 256^2 plane spills even at 255 registers: generic)
+    A_ENTRY(double, 1, 128, 64, 4, 8, 256, 0, 0, 1),
 };
 const int kNumVariantsA_f64 = sizeof(kVariantsA_f64) / sizeof(kVariantsA_f64[0]);
 
@@ -18,6 +23,13 @@ const VariantB kVariantsB_f64[] = {
     B_ENTRY(double, 1, 512, 8, 256, 0, 2),
     B_ENTRY(double, 1, 512, 4, 256, 0, 2),
     B_ENTRY(double, 1, 128, 8, 256, 0, 2),
+    // 1024 (8 x 16-byte complex = 128-byte tile rows), 384, 256
+    B_ENTRY(double, 1, 1024, 8, 512, 0, 1),
+    B_ENTRY(double, 1, 1024, 4, 256, 0, 1),
+    P_ENTRY(double, 1, 384, 8, 256, 0, 1),
+    B_ENTRY(double, 1, 384, 8, 256, 0, 1),
+    P_ENTRY(double, 1, 256, 8, 256, 0, 1),
+    B_ENTRY(double, 1, 256, 8, 256, 0, 1),
 };
 const int kNumVariantsB_f64 = sizeof(kVariantsB_f64) / sizeof(kVariantsB_f64[0]);
 
