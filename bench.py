@@ -380,9 +380,10 @@ def run_reference(args, world, rank):
             "data": "synthetic: seeded i.i.d. N(0,1) real field, padded layout",
             "config": {"workload": f"in-place R2C+C2R, {nx}x{ny}x{nz} {dt}, procs=1 per GPU", "grid": [nx, ny, nz],
                        "field_bytes": S, "parallelism": f"replicas x{world}"}}
+    if rank != 0:
+        return None  # under torchrun the reference arm runs on rank 0 alone; the other ranks exit
+    base["config"]["parallelism"] = "rank 0 alone (reference arm)"
     if not os.path.exists(lib_path):
-        if rank != 0:
-            return None
         cb = cpu_baseline(nx, ny, nz)
         base.update({"value": round(cb["value"], 3), "ms_per_step": round(cb["value"], 3), "cpu_baseline": cb,
                      "e2e": {"value": round(cb["value"], 3), "unit": "ms", "h2d_bytes_per_step": 0,
@@ -414,11 +415,11 @@ def run_reference(args, world, rank):
     while done < args.steps:
         k = min(4, args.steps - done)
         f.mul_(scale)
-        t, p = time_steps(step, k, 0, world, stream)
+        t, p = time_steps(step, k, 0, 1, stream)
         total_ms += t
         per += p
         done += k
-    ms = max_over_ranks(world, total_ms / args.steps)
+    ms = total_ms / args.steps
     host_in = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
     host_in.copy_(f.cpu())
     host_out = torch.empty_like(host_in, pin_memory=True)
@@ -430,10 +431,8 @@ def run_reference(args, world, rank):
         host_out.copy_(f, non_blocking=True)
 
     e_steps = max(3, min(args.steps, 10))
-    e_total, _ = time_steps(e2e_step, e_steps, 2, world, stream)
-    e2e_ms = max_over_ranks(world, e_total / e_steps)
-    if rank != 0:
-        return None
+    e_total, _ = time_steps(e2e_step, e_steps, 2, 1, stream)
+    e2e_ms = e_total / e_steps
     base.update({
         "value": round(ms, 4), "ms_per_step": round(ms, 4), "p50_ms": round(pct(per, 50), 4),
         "p99_ms": round(pct(per, 99), 4),
