@@ -310,7 +310,7 @@ def run_ours(args, world, rank):
     if (nx, ny, nz, dt) == (512, 512, 512, "float") and dom == "pass_A_fwd" and \
             "fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4 " in plan.describe() and \
             "split=0}" in plan.describe():
-        traffic = 558_529_024 + 766_980_864
+        traffic = 560_384_512 + 771_755_008
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
                 "algorithmic_bytes_per_launch": 2 * S, "peak_source": peak_kind,

@@ -448,3 +448,33 @@ def test_pass_a_cluster_size_does_not_change_results(cuda, tmp_path, k):
     # leave the process-wide wisdom at the defaults for the tests that follow
     path.write_text(f"{dev}_sm{major * 10 + minor} 0 {n} {n} {n} 0 0 0\n")
     g.wisdom_load(str(path))
+
+
+def _golden_cases():
+    path = os.path.join(ROOT, "tests", "golden", "ref_cufft_golden.npz")
+    if not os.path.exists(path):
+        return []
+    with np.load(path) as z:
+        return sorted({k.rsplit("__", 1)[0] for k in z.files})
+
+
+@pytest.mark.parametrize("case", _golden_cases())
+def test_matches_reference_outputs_directly(oracle, cuda, case):
+    """Our R2C and C2R of the same inputs against the outputs the reference
+    itself (GPU_FFT at procs=1, cuFFT) produced on a B200
+    (tests/golden/ref_cufft_golden.npz): R2C within the FP32/FP64 bar, and our
+    C2R of the reference's spectrum within the bar of the reference's C2R."""
+    import json
+
+    import torch
+
+    with np.load(os.path.join(ROOT, "tests", "golden", "ref_cufft_golden.npz")) as z:
+        meta = json.loads(str(z[case + "__meta"]))
+        ref_r2c = z[case + "__r2c"]
+        ref_c2r = z[case + "__c2r"]
+    nx, ny, nz, dt = meta["nx"], meta["ny"], meta["nz"], meta["dtype"]
+    f = oracle.uniform_field(nx, ny, nz, seed=meta["seed"], dtype=NPDT[dt])
+    got = run_r2c(f, (nx, ny, nz), dt)
+    assert oracle.rel_l2(got, ref_r2c) < TOL[dt]
+    back = run_c2r(ref_r2c, (nx, ny, nz), dt)
+    assert oracle.rel_l2(back[:, :, :nz], ref_c2r[:, :, :nz]) < TOL[dt]
