@@ -590,27 +590,66 @@ def run_precision(args, world, rank):
     y32 = x32.clone()
     p32.r2c(y32)
     e_l2, e_max = errors(y32)
-    del y32
-    ptr = x32.data_ptr()
 
-    def step32():
-        p32.r2c_ptr(ptr, sh)
-        p32.c2r_ptr(ptr, sh)
+    def time_fp32_plan(plan, x):
+        ptr = x.data_ptr()
 
-    total, done = 0.0, 0
-    for _ in range(args.warmup):
-        x32.mul_(1.0 / n ** 3)
-        step32()
-    while done < args.steps:
-        k = min(4, args.steps - done)
-        x32.mul_(1.0 / n ** 3)
-        t, _ = time_steps(step32, k, 0, world, stream)
-        total += t
-        done += k
-    ms32 = total / args.steps
+        def step32():
+            plan.r2c_ptr(ptr, sh)
+            plan.c2r_ptr(ptr, sh)
+
+        total, done = 0.0, 0
+        for _ in range(args.warmup):
+            x.mul_(1.0 / n ** 3)
+            step32()
+        while done < args.steps:
+            k = min(4, args.steps - done)
+            x.mul_(1.0 / n ** 3)
+            t, _ = time_steps(step32, k, 0, world, stream)
+            total += t
+            done += k
+        return total / args.steps
+
+    def time_x_pass(plan, x):
+        """ms of one x-pass launch (mean of forward and inverse): the pass
+        whose radix-16 stages the tensor-core form changes"""
+        ptr = x.data_ptr()
+
+        def stepb():
+            plan.pass_ptr(ptr, sh, 1, True)
+            plan.pass_ptr(ptr, sh, 1, False)
+
+        x.mul_(1.0 / n)
+        t, _ = time_steps(stepb, 4, 2, world, stream)
+        return t / 8
+
+    ms32 = time_fp32_plan(p32, x32)
     out["fp32"] = {"ms": round(ms32, 4), "rel_l2_vs_fp64": e_l2, "max_err_rel_to_max": e_max,
-                   "field_bytes": S32}
+                   "field_bytes": S32, "x_pass_ms": round(time_x_pass(p32, x32), 4), "plan": p32.describe()}
     del x32
+    # ---- FP32 storage, x-pass radix-16 stages on the tensor cores (split BF16)
+    try:
+        ptc = g.Plan(n, n, n, "float", autotune=not args.no_autotune, tc_split=True)
+    except g.GpuFFTError as e:
+        out["tc_split_bf16"] = {"status": f"unsupported at {n}^3: {e}"}
+        ptc = None
+    if ptc is not None:
+        xt = f64.float()
+        yt = xt.clone()
+        ptc.r2c(yt)
+        t_l2, t_max = errors(yt)
+        vs_plain = ((yt.double() - y32.double()).norm() / y32.double().norm()).item()
+        del yt
+        mst = time_fp32_plan(ptc, xt)
+        xb = time_x_pass(ptc, xt)
+        out["tc_split_bf16"] = {"ms": round(mst, 4), "rel_l2_vs_fp64": t_l2, "max_err_rel_to_max": t_max,
+                                "rel_l2_vs_plain_fp32": vs_plain, "gate_vs_plain": 1e-6,
+                                "speedup_vs_fp32": round(ms32 / mst, 3), "field_bytes": S32,
+                                "x_pass_ms": round(xb, 4),
+                                "x_pass_speedup_vs_fp32": round(out["fp32"]["x_pass_ms"] / xb, 3),
+                                "plan": ptc.describe()}
+        del xt, ptc
+    del y32
     # ---- 16-bit storage, per-pencil scales, FP32 butterflies
     for fmt in ("bf16", "fp16"):
         p16 = g.Plan16(n, n, n, fmt)
@@ -645,7 +684,6 @@ def run_precision(args, world, rank):
         out[fmt] = {"ms": round(ms16, 4), "rel_l2_vs_fp64": e_l2, "max_err_rel_to_max": e_max,
                     "field_bytes": S32 // 2, "speedup_vs_fp32": round(ms32 / ms16, 3)}
         del p16, field, scales
-    out["tc_split_bf16"] = {"status": "not built: the radix-16 stages run on the FP32 pipes"}
     if rank != 0:
         return None
     peak, _ = load_peaks()

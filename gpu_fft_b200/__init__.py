@@ -41,6 +41,7 @@ EXPORTS = (
     "gpufft_dplan_layout", "gpufft_dgroup_create", "gpufft_dgroup_exec",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
+GPUFFT_PLAN_TC_SPLIT = 2
 
 _lib = None
 
@@ -175,12 +176,14 @@ def field_bytes(nx: int, ny: int, nz: int, dtype="float") -> int:
 class Plan:
     """A plan for one grid and precision (gpufft_plan_create)."""
 
-    def __init__(self, nx: int, ny: int, nz: int, dtype="float", autotune: bool = False):
+    def __init__(self, nx: int, ny: int, nz: int, dtype="float", autotune: bool = False, tc_split: bool = False):
+        """`tc_split`: run the x pass's radix-16 stages on the tensor cores
+        (split BF16 operands, FP32 accumulation; FP32 plans, Nx = 512, 1024)."""
         lib = load_library()
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dtype_code = _dtype_code(dtype)
         h = ctypes.c_void_p()
-        flags = GPUFFT_PLAN_AUTOTUNE if autotune else 0
+        flags = (GPUFFT_PLAN_AUTOTUNE if autotune else 0) | (GPUFFT_PLAN_TC_SPLIT if tc_split else 0)
         _check(lib.gpufft_plan_create_ex(ctypes.byref(h), self.nx, self.ny, self.nz, self.dtype_code, flags))
         self._h = h
 

@@ -52,6 +52,12 @@ const VariantB kVariantsB_f32[] = {
     B_ENTRY(float, 0, 128, 16, 256, 0, 2),
     B_ENTRY(float, 0, 96, 16, 256, 0, 2),
     B_ENTRY(float, 0, 64, 16, 256, 0, 2),
+    // tensor-core radix-16 stages (v = 2): only plans made with
+    // GPUFFT_PLAN_TC_SPLIT use these, and they use nothing else
+    P_ENTRY(float, 0, 512, 16, 512, 2, 1),
+    P_ENTRY(float, 0, 512, 16, 256, 2, 2),
+    B_ENTRY(float, 0, 512, 16, 256, 2, 2),
+    B_ENTRY(float, 0, 1024, 16, 512, 2, 1),
 };
 const int kNumVariantsB_f32 = sizeof(kVariantsB_f32) / sizeof(kVariantsB_f32[0]);
 

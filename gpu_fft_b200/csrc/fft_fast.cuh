@@ -14,6 +14,7 @@
 //    instead of 8.
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include <type_traits>
 
@@ -27,7 +28,9 @@ namespace fast {
 // compile-time radix lists (same rule as the host factorize(): the power of
 // two split into balanced stages of at most 16, then pairs of 3s as radix 9,
 // then odd primes 3..13).
-// VARIANT 1 prefers radix-16 stages for the power-of-two part.
+// VARIANT 1 prefers radix-16 stages for the power-of-two part; VARIANT 2 has
+// the same radix list and runs the radix-16 stages of FP32 column tiles on
+// the tensor cores (split BF16, TileFFT::stage_tc16).
 // ---------------------------------------------------------------------------
 struct Fac {
     int n;
@@ -42,7 +45,7 @@ __host__ __device__ constexpr Fac factor(int N, int variant) {
         ++a;
     }
     if (a > 0) {
-        if (variant == 1) {
+        if (variant >= 1) {
             int left = a;
             while (left >= 4) {
                 f.r[f.n++] = 16;
@@ -99,18 +102,66 @@ enum Scope { BLOCK = 0, WARP = 1 };
 //        conflict-free); PITCH keeps rows apart by an odd number of slots
 enum Layout { COLS = 0, ROWS = 1 };
 
-template <typename T, int N, int W, int LAYOUT>
+//  TC (COLS, W = 16, FP32, tensor-core radix-16 stages): column pairs are
+//        XOR-swizzled by row bits, w ^ sw(n), so the fragment-shaped loads
+//        and stores of TileFFT::stage_tc16 are conflict-free (a whole row is
+//        still a permutation of its 16 columns, and a 16-byte pair stays
+//        together):
+//          sw bit 2 = n bit B, sw bit 3 = n bit B+1 ^ n bits log2(p_s),
+//        with 2^B = 2 N/16 (the loads of a radix-16 stage touch rows
+//        i + (2t + c) N/16, t = lane % 4) and p_s the sub-length of each
+//        tensor-core stage s (its stores touch rows o + g p_s, g = lane / 4).
+template <typename T, int N, int W, int LAYOUT, bool TC = false>
 struct TileLayout {
     using V = cx_t<T>;
     static constexpr int G = 128 / (int)sizeof(V);
     static constexpr int ROWLEN = N + (N + G - 1) / G;
     static constexpr int PITCH = (ROWLEN % 2 == 0) ? ROWLEN + 1 : ROWLEN;
     static constexpr int ELEMS = LAYOUT == COLS ? N * W : W * PITCH;
+    static constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
+    static constexpr int SWB = ilog2(N / 8);
+    // rows whose bit log2(p_s) feeds sw bit 3: the radix-16 stages but the last
+    static constexpr unsigned pmask() {
+        const Fac f = factor(N, 2);
+        unsigned m = 0;
+        int p = 1;
+        for (int s = 0; s + 1 < f.n; ++s) {
+            if (f.r[s] == 16) m |= (unsigned)p;
+            p *= f.r[s];
+        }
+        return m;
+    }
+    static constexpr unsigned PMASK = pmask();
+    static constexpr bool kSw = LAYOUT == COLS && TC;
+    static __host__ __device__ constexpr int parity(unsigned v) {
+        v ^= v >> 16;
+        v ^= v >> 8;
+        v ^= v >> 4;
+        v ^= v >> 2;
+        v ^= v >> 1;
+        return (int)(v & 1u);
+    }
+    static __host__ __device__ constexpr int swz(int n) {
+        const int b3 = (parity((unsigned)n & PMASK) ^ (n >> (SWB + 1))) & 1;
+        return (((n >> SWB) & 1) << 2) | (b3 << 3);
+    }
     static __device__ __forceinline__ int idx(int n, int w) {
-        if constexpr (LAYOUT == COLS)
+        if constexpr (LAYOUT == COLS && TC)
+            return n * W + (w ^ swz(n));
+        else if constexpr (LAYOUT == COLS)
             return n * W + w;
         else
             return w * PITCH + n + n / G;
+    }
+    // idx(a + b, w) for a and b without common set bits (a stage's row
+    // i + j*nb with i < nb, or o + j*p, for power-of-two lengths): the
+    // swizzle is XOR-linear in the row bits, so sw(a + b) = sw(a) ^ sw(b),
+    // and with b a compile-time multiple after unrolling, sw(b) folds away
+    static __device__ __forceinline__ int idx_sum(int a, int b, int w) {
+        if constexpr (LAYOUT == COLS && TC)
+            return (a + b) * W + (w ^ swz(a) ^ swz(b));
+        else
+            return idx(a + b, w);
     }
 };
 
@@ -123,7 +174,10 @@ struct ToSmem {};
 template <typename T, int N, int W, int NT, bool FWD, int LAYOUT, int VARIANT = 0, int SCOPE = BLOCK>
 struct TileFFT {
     using V = cx_t<T>;
-    using L = TileLayout<T, N, W, LAYOUT>;
+    static constexpr bool kTcStage = VARIANT == 2 && std::is_same<T, float>::value && LAYOUT == COLS &&
+                                     SCOPE == BLOCK && W == 16 && NT >= 64 && (N & (N - 1)) == 0 &&
+                                     (NT & (NT - 1)) == 0;
+    using L = TileLayout<T, N, W, LAYOUT, kTcStage>;
     static constexpr Fac F = factor(N, VARIANT);
     static constexpr int NS = F.n;
     static_assert(NS >= 0, "length must factor into 2,3,5,7,11,13");
@@ -142,8 +196,188 @@ struct TileFFT {
             return (int)threadIdx.x;
     }
 
+    // ---- radix-16 stage on the tensor cores (VARIANT 2: FP32 column tiles
+    // of width 16, whole CTA; every radix-16 stage but the last).
+    // The 16-point DFTs of 8 butterflies (same i, 8 adjacent columns) are one
+    // 16x16 by 16x8 product Y = F X, done by mma.sync.m16n8k16 with BF16
+    // operands and FP32 accumulation.  Each FP32 value (the DFT entries, and
+    // the inputs after their twiddle) is split into three BF16 terms
+    // h + m + l (8 significant bits each, 24 together); the six products
+    // with term orders adding up to at most 2 are kept (hh; hm, mh; hl, mm,
+    // lh), smallest first, so the result carries about FP32's precision.
+    // Complex arithmetic as real products: Yr = Fr Xr + Fi (-Xi),
+    // Yi = Fr Xi + Fi Xr (24 MMAs per 8 butterflies).
+    // Fragment layouts (PTX ISA, m16n8k16 .row.col), with g = lane/4 and
+    // t = lane%4: A[g(+8)][2t(+1)(+8)], B[2t(+1)(+8)][g], D[g(+8)][2t(+1)].
+    struct Split3 {
+        uint32_t h, m, l;  // packed BF16 pairs (low half = first value)
+    };
+    static __device__ __forceinline__ uint32_t bf16x2(float a, float b) {
+        const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+        uint32_t u;
+        memcpy(&u, &v, 4);
+        return u;
+    }
+    // the BF16 pair u widened back to two FP32 values (exact)
+    static __device__ __forceinline__ float lo_f(uint32_t u) { return __uint_as_float(u << 16); }
+    static __device__ __forceinline__ float hi_f(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+    static __device__ __forceinline__ Split3 split3(float a, float b) {
+        Split3 s;
+        s.h = bf16x2(a, b);
+        const float ra = a - lo_f(s.h), rb = b - hi_f(s.h);  // exact remainders
+        s.m = bf16x2(ra, rb);
+        s.l = bf16x2(ra - lo_f(s.m), rb - hi_f(s.m));
+        return s;
+    }
+    static __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    }
+    // cos(2 pi m / 16), m = 0..15, from the exact values of cos(k pi / 8)
+    static __device__ __forceinline__ float cos16(int m) {
+        const float c1 = 0.92387953251128675613f, c2 = 0.70710678118654752440f, c3 = 0.38268343236508977173f;
+        const int q = m & 7;  // cos(x + pi) = -cos(x)
+        const int r = q <= 4 ? q : 8 - q;
+        const float v = r == 0 ? 1.f : r == 1 ? c1 : r == 2 ? c2 : r == 3 ? c3 : 0.f;
+        return ((m & 8) != 0) != (q > 4) ? -v : v;
+    }
+    // A fragments of the DFT-16 matrix F[r][c] = exp(-+ 2 pi i r c / 16),
+    // real and imaginary parts, three BF16 terms each.  Only a0 (F[g][2t],
+    // F[g][2t+1]) is kept: F[r+8][c] = (-1)^c F[r][c] and F[r][c+8] =
+    // (-1)^r F[r][c], so a1..a3 are a0 with sign bits flipped (exact, as
+    // the split of -x is minus the split of x).
+    struct DftFrag {
+        uint32_t re[3], im[3];
+    };
+    static __device__ __forceinline__ DftFrag dft16_fragments() {
+        DftFrag f;
+        const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+        const int m0 = (g * 2 * t) & 15, m1 = (g * (2 * t + 1)) & 15;
+        // sin(x) = cos(x - pi/2); forward transform: exp(-i x)
+        const float s0 = cos16((m0 + 12) & 15), s1 = cos16((m1 + 12) & 15);
+        const Split3 re = split3(cos16(m0), cos16(m1));
+        const Split3 im = FWD ? split3(-s0, -s1) : split3(s0, s1);
+        f.re[0] = re.h;
+        f.re[1] = re.m;
+        f.re[2] = re.l;
+        f.im[0] = im.h;
+        f.im[1] = im.m;
+        f.im[2] = im.l;
+        return f;
+    }
+    // D += A(a0) B, with A's other three registers derived from a0
+    static __device__ __forceinline__ void mma_dft(float (&d)[4], uint32_t a0, uint32_t sg, uint32_t b0, uint32_t b1) {
+        const uint32_t a[4] = {a0, a0 ^ 0x80000000u, a0 ^ sg, a0 ^ sg ^ 0x80000000u};
+        mma_bf16(d, a, b0, b1);
+    }
+
+    // Work split: warp wp takes butterflies i = wp/2 + u*NWARP/2 (u = 0, 1,
+    // ...) in columns (wp%2)*8 .. +7.  Every tile row index below is a sum of
+    // parts without common bits -- a per-thread part (wp/2, t or g) and a
+    // compile-time part (u, the input or output slot) -- so the swizzle of
+    // a row is the XOR of per-thread constants and folded constants.
+    template <int S, class Src, class Dst>
+    static __device__ __forceinline__ void stage_tc16(Src &src, Dst &dst, V *sm, const V *tw) {
+        constexpr int R = 16;
+        constexpr int p = fac_prod(F, S);
+        constexpr int nb = N / R;
+        constexpr bool src_smem = S != 0 || std::is_same<Src, FromSmem>::value;
+        constexpr int NWARP = NT / 32;
+        constexpr int HB = NWARP / 2;  // butterfly rows i per u step
+        constexpr int GPW = (nb + HB - 1) / HB;
+        static_assert(S < NS - 1, "the last stage runs on the FP32 pipes");
+        static_assert(p == 1 || p >= HB, "k = i mod p splits into per-thread and compile-time parts");
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+        const int a = warp >> 1;           // per-thread part of i (< HB)
+        const int w0 = (warp & 1) * 8;     // first column of the warp's butterflies
+        const DftFrag fr = dft16_fragments();
+        const uint32_t sg = (g & 1) ? 0x80008000u : 0u;  // (-1)^g on both halves
+        V x[GPW][4];
+        if (src_smem) sync();
+        {
+            // input rows i + j*nb, j = 2t + c (c = 0, 1, 8, 9)
+            const int sw_ld = L::swz(a) ^ L::swz(2 * t * nb);
+#pragma unroll
+            for (int u = 0; u < GPW; ++u) {
+                if ((u + 1) * HB <= nb || a + u * HB < nb) {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int c = (e & 1) + ((e & 2) ? 8 : 0);
+                        const int row = a + u * HB + (2 * t + c) * nb;
+                        if constexpr (src_smem)
+                            x[u][e] = sm[row * W + ((w0 + g) ^ sw_ld ^ L::swz(u * HB + c * nb))];
+                        else
+                            x[u][e] = src(row, w0 + g);
+                    }
+                }
+            }
+        }
+        sync();  // every reader of the tile is done before it is overwritten
+        // output rows o + jout*p, o = (i - k)*R + k, k = i mod p
+        constexpr int ao_mul = p == 1 ? R : 1;  // per-thread part of o: a*R (p = 1) or a
+        const int sw_st = L::swz(a * ao_mul) ^ L::swz(g * p);
+#pragma unroll
+        for (int u = 0; u < GPW; ++u) {
+            if ((u + 1) * HB <= nb || a + u * HB < nb) {
+                const int b = u * HB;                           // compile-time part of i
+                const int bk = p == 1 ? 0 : b % p;              // compile-time part of k
+                const int k = p == 1 ? 0 : a + bk;
+                const int oc = p == 1 ? b * R : (b - bk) * R + bk;  // compile-time part of o
+                if constexpr (p > 1) {
+                    constexpr int off = stage_offset(F, S);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int j = 2 * t + (e & 1) + ((e & 2) ? 8 : 0);
+                        if (j > 0) x[u][e] = c_tw<FWD>(x[u][e], tw[off + (j - 1) * p + k]);
+                    }
+                }
+                // B fragments: b0 = rows 2t, 2t+1; b1 = rows 2t+8, 2t+9 (column g)
+                const Split3 r0 = split3(x[u][0].x, x[u][1].x), r1 = split3(x[u][2].x, x[u][3].x);
+                const Split3 i0 = split3(x[u][0].y, x[u][1].y), i1 = split3(x[u][2].y, x[u][3].y);
+                const uint32_t xr[3][2] = {{r0.h, r1.h}, {r0.m, r1.m}, {r0.l, r1.l}};
+                const uint32_t xi[3][2] = {{i0.h, i1.h}, {i0.m, i1.m}, {i0.l, i1.l}};
+                constexpr uint32_t NEG = 0x80008000u;
+                float yr[4] = {0.f, 0.f, 0.f, 0.f}, yi[4] = {0.f, 0.f, 0.f, 0.f};
+                // term pairs (F term, X term), smallest first
+                constexpr int ta[6] = {0, 1, 2, 0, 1, 0}, tb[6] = {2, 1, 0, 1, 0, 0};
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const int fa = ta[q], xb = tb[q];
+                    mma_dft(yr, fr.re[fa], sg, xr[xb][0], xr[xb][1]);
+                    mma_dft(yr, fr.im[fa], sg, xi[xb][0] ^ NEG, xi[xb][1] ^ NEG);
+                    mma_dft(yi, fr.re[fa], sg, xi[xb][0], xi[xb][1]);
+                    mma_dft(yi, fr.im[fa], sg, xr[xb][0], xr[xb][1]);
+                }
+                // D: outputs jout = g (d0, d1) and g + 8 (d2, d3) of the
+                // butterflies in columns w0 + 2t and w0 + 2t + 1, stored as
+                // one 16-byte pair per output row
+                const int row = a * ao_mul + oc + g * p;
+                const int col = (w0 + 2 * t) ^ sw_st ^ L::swz(oc);
+                st_pair(sm, row * W + col, V{yr[0], yi[0]}, V{yr[1], yi[1]});
+                st_pair(sm, (row + 8 * p) * W + (col ^ L::swz(8 * p)), V{yr[2], yi[2]}, V{yr[3], yi[3]});
+            }
+        }
+    }
+    // two adjacent complex values at an even tile index (16-byte aligned)
+    static __device__ __forceinline__ void st_pair(V *sm, int idx, V a, V b) {
+        *reinterpret_cast<float4 *>(sm + idx) = make_float4(a.x, a.y, b.x, b.y);
+    }
+
     template <int S, class Src, class Dst>
     static __device__ __forceinline__ void stage(Src &src, Dst &dst, V *sm, const V *tw) {
+        if constexpr (kTcStage && F.r[S] == 16 && S < NS - 1) {
+            stage_tc16<S>(src, dst, sm, tw);
+            return;
+        } else {
+            stage_scalar<S>(src, dst, sm, tw);
+        }
+    }
+
+    template <int S, class Src, class Dst>
+    static __device__ __forceinline__ void stage_scalar(Src &src, Dst &dst, V *sm, const V *tw) {
         constexpr int R = F.r[S];
         constexpr int p = fac_prod(F, S);
         constexpr int nb = N / R;
@@ -173,8 +407,10 @@ struct TileFFT {
                 ww[m] = w;
 #pragma unroll
                 for (int j = 0; j < R; ++j) {
-                    if constexpr (src_smem)
-                        v[m][j] = sm[L::idx(i + j * nb, w)];
+                    if constexpr (src_smem && L::kSw)  // i = tid/W + m*NT/W (disjoint bits)
+                        v[m][j] = sm[L::idx_sum(tid / W, m * (NT / W) + j * nb, w)];
+                    else if constexpr (src_smem)
+                        v[m][j] = sm[L::idx_sum(i, j * nb, w)];
                     else
                         v[m][j] = src(i + j * nb, w);
                 }
@@ -211,15 +447,17 @@ struct TileFFT {
                     // last stage: p = nb, k = i, output positions i + j*nb
 #pragma unroll
                     for (int j = 0; j < R; ++j) {
-                        if constexpr (dst_smem)
-                            sm[L::idx(i + j * nb, w)] = v[m][j];
+                        if constexpr (dst_smem && L::kSw)
+                            sm[L::idx_sum(tid / W, m * (NT / W) + j * nb, w)] = v[m][j];
+                        else if constexpr (dst_smem)
+                            sm[L::idx_sum(i, j * nb, w)] = v[m][j];
                         else
                             dst(i + j * nb, w, v[m][j]);
                     }
                 } else {
                     const int o = (i - k) * R + k;
 #pragma unroll
-                    for (int j = 0; j < R; ++j) sm[L::idx(o + j * p, w)] = v[m][j];
+                    for (int j = 0; j < R; ++j) sm[L::idx_sum(o, j * p, w)] = v[m][j];
                 }
             }
         }
@@ -341,7 +579,7 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_pipe(PassBParams P) {
             const int w = ch * PER16;
             const int valid = max(0, min(PER16, wv - w));
             const V *src = base + (long long)n * ncols + c0 + (valid > 0 ? w : 0);
-            cp_async16(buf + n * W + w, src, valid * (int)sizeof(V));
+            cp_async16(buf + FFT::L::idx(n, w), src, valid * (int)sizeof(V));
         }
         cp_async_commit();
     };

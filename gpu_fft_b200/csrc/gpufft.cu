@@ -238,6 +238,15 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
     return dtype == GPUFFT_FLOAT ? f32 : f64;
 }
 
+// A Pass B entry serves this plan: its length, 16-byte tile rows for the
+// cp.async form, and tensor-core stages (v = 2) exactly when the plan asks
+// for them.
+static bool b_eligible(const Plan &P, const fast::VariantB &v) {
+    const int m = (int)(P.nz / 2);
+    const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
+    return v.nx == (int)P.nx && (v.kind != 1 || rows16) && ((v.v == 2) == P.tc_split);
+}
+
 // Picks the specialised kernels for this plan's shape (first registry entry,
 // or the entries named by the autotuner) and sizes their launches.
 static int setup_fast(Plan &P, int idx_a, int idx_b) {
@@ -256,9 +265,8 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
     for (int i = 0; i < na && !P.fa; ++i)
         if (va[i].ny == ny && va[i].m == m && seen++ == idx_a) P.fa = &va[i];
     seen = 0;
-    const bool rows16 = ((long long)ny * (m + 1) * vs) % 16 == 0;  // cp.async tiles need 16-byte row starts
     for (int i = 0; i < nb && !P.fb; ++i)
-        if (vb[i].nx == nx && (vb[i].kind != 1 || rows16) && seen++ == idx_b) P.fb = &vb[i];
+        if (b_eligible(P, vb[i]) && seen++ == idx_b) P.fb = &vb[i];
     if (P.fa) {
         for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
             cudaError_t e = raise_smem_limit(k, P.fa->smem);
@@ -350,8 +358,10 @@ static std::string device_tag(int dev) {
     return name + "_sm" + std::to_string(prop.major * 10 + prop.minor);
 }
 
+// tensor-core plans are remembered apart from plain ones (dtype + 16)
 static WisdomKey wisdom_key(const Plan &P) {
-    return WisdomKey(device_tag(P.device), P.dtype, (long long)P.nx, (long long)P.ny, (long long)P.nz);
+    return WisdomKey(device_tag(P.device), P.dtype + (P.tc_split ? 16 : 0), (long long)P.nx, (long long)P.ny,
+                     (long long)P.nz);
 }
 
 static int wisdom_load_locked(const char *path) {
@@ -419,7 +429,7 @@ static void wisdom_store(const Plan &P) {
 }
 
 static int count_candidates(const Plan &P, int pass) {
-    const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
+    const int ny = (int)P.ny, m = (int)(P.nz / 2);
     int n = 0;
     if (pass == 0) {
         const fast::VariantA *va = variants_a(P.dtype).data();
@@ -428,8 +438,7 @@ static int count_candidates(const Plan &P, int pass) {
     } else {
         const fast::VariantB *vb = variants_b(P.dtype).data();
         const int nb = (int)variants_b(P.dtype).size();
-        const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
-        for (int i = 0; i < nb; ++i) n += (vb[i].nx == nx && (vb[i].kind != 1 || rows16));
+        for (int i = 0; i < nb; ++i) n += b_eligible(P, vb[i]);
     }
     return n;
 }
@@ -477,7 +486,8 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
     for (int pass = 0; pass < 2; ++pass) {
         const int n = count_candidates(*P, pass);
         float best_ms = 1e30f;
-        for (int c = -1; c < n; ++c) {
+        // (a tensor-core plan's x pass is one of its v = 2 kernels, never generic)
+        for (int c = (pass == 1 && P->tc_split) ? 0 : -1; c < n; ++c) {
             // Pass A candidates are timed at the cluster size chosen from the
             // L2 size (K), at K/2 and K/4, at 16 when K is 8, and split into
             // two launches
@@ -628,7 +638,7 @@ static int build_plan(Plan &P) {
     P.grid_b = (int)std::min<long long>(B.ntiles, (long long)occ_b * sms);
     P.occ_a = occ_a;
     P.occ_b = occ_b;
-    if (std::getenv("GPUFFT_GENERIC_ONLY")) {
+    if (std::getenv("GPUFFT_GENERIC_ONLY") && !P.tc_split) {
         P.idx_a = P.idx_b = -1;
         return GPUFFT_SUCCESS;
     }
@@ -637,7 +647,11 @@ static int build_plan(Plan &P) {
     const char *va = std::getenv("GPUFFT_VARIANT_A"), *vb = std::getenv("GPUFFT_VARIANT_B");
     if (va) ia = std::atoi(va);
     if (vb) ib = std::atoi(vb);
-    return setup_fast(P, ia, ib);
+    const int rc = setup_fast(P, ia, ib);
+    if (rc == GPUFFT_SUCCESS && P.tc_split && !P.fb)
+        return set_error(GPUFFT_ERR_UNSUPPORTED,
+                         "no tensor-core x-pass kernel for Nx=%lld (compiled: FP32, Nx = 512 and 1024)", (long long)nx);
+    return rc;
 }
 
 int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags) {
@@ -655,6 +669,11 @@ int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int f
     Plan *P = new (std::nothrow) Plan();
     if (!P) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
     P->nx = nx; P->ny = ny; P->nz = nz; P->dtype = dtype;
+    P->tc_split = (flags & GPUFFT_PLAN_TC_SPLIT) != 0;
+    if (P->tc_split && dtype != GPUFFT_FLOAT) {
+        delete P;
+        return set_error(GPUFFT_ERR_UNSUPPORTED, "GPUFFT_PLAN_TC_SPLIT is an FP32 form");
+    }
     cudaError_t e = cudaGetDevice(&P->device);
     if (e != cudaSuccess) { delete P; return cuda_error(e, "cudaGetDevice"); }
     const int rc = dtype == GPUFFT_FLOAT ? build_plan<float>(*P) : build_plan<double>(*P);

@@ -30,6 +30,7 @@ struct Plan {
     int kfix = 0;              // specialised Pass A cluster size (0: chosen from the L2 size;
                                // -1: split Pass A, z rows and y columns in two launches)
     bool split_a = false;      // specialised Pass A runs as two launches (kfix == -1)
+    bool tc_split = false;     // x pass on the tensor-core radix-16 kernels (GPUFFT_PLAN_TC_SPLIT)
     bool tuned = false;
 };
 

@@ -123,6 +123,13 @@ int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int f
  * and autotuning appends to it.
  * ------------------------------------------------------------------------ */
 #define GPUFFT_PLAN_AUTOTUNE 1
+/* FP32 plans only: the x pass runs its radix-16 stages as 16x16 DFT-matrix
+ * products on the tensor cores (mma.sync, BF16 operands split into three
+ * terms, FP32 accumulation; within about 1e-7 relative L2 of the plain FP32
+ * plan).  Compiled for Nx = 512 and 1024; other Nx give
+ * GPUFFT_ERR_UNSUPPORTED.  No reference counterpart (GPU_FFT's transforms
+ * are cuFFT's). */
+#define GPUFFT_PLAN_TC_SPLIT 2
 
 int gpufft_plan_create_ex(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);
 
