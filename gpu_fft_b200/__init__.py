@@ -32,7 +32,8 @@ EXPORTS = (
     "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
     "gpufft_exec_noalloc",
     "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
-    "gpufft_batch_status", "gpufft_batch_items",
+    "gpufft_batch_status", "gpufft_batch_items", "gpufft_batch_set_schedule", "gpufft_batch_schedule",
+    "gpufft_batch_autotune",
     "gpufft_plan16_create", "gpufft_plan16_destroy", "gpufft_plan16_scale_count", "gpufft_exec16_r2c",
     "gpufft_exec16_c2r", "gpufft_exec16_pass", "gpufft_quantize16", "gpufft_dequantize16",
     "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
@@ -103,6 +104,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_batch_exec_graph.argtypes = [vp, ctypes.POINTER(vp), vp]
     lib.gpufft_batch_status.argtypes = [vp, vp]
     lib.gpufft_batch_items.argtypes = [vp]
+    lib.gpufft_batch_set_schedule.argtypes = [vp, ci, ci]
+    lib.gpufft_batch_schedule.argtypes = [vp, ctypes.POINTER(ci), ctypes.POINTER(ci)]
+    lib.gpufft_batch_autotune.argtypes = [vp, vp]
     lib.gpufft_plan16_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci]
     lib.gpufft_plan16_destroy.argtypes = [vp]
     lib.gpufft_plan16_scale_count.argtypes = [vp]
@@ -259,12 +263,19 @@ class Plan:
             pass
 
 
+GPUFFT_BATCH_PERSISTENT = 0
+GPUFFT_BATCH_BRANCHES = 1
+
+
 class Batch:
     """Many independent in-place transforms (mixed grids, each R2C or C2R) in one
-    persistent kernel launch (gpufft_batch_*).  grids: list of (Nx, Ny, Nz);
-    directions: list of "r2c"/"c2r" (or 1/0)."""
+    call (gpufft_batch_*).  grids: list of (Nx, Ny, Nz); directions: list of
+    "r2c"/"c2r" (or 1/0).  schedule: "persistent" (one persistent kernel
+    launch), "branches" (each transform's own specialised kernels on
+    `branches` concurrent streams) or "auto" (gpufft_batch_autotune: tune the
+    plans, time both on scratch fields, keep the faster)."""
 
-    def __init__(self, grids, directions, dtype="float"):
+    def __init__(self, grids, directions, dtype="float", schedule="persistent", branches=4, stream=None):
         lib = load_library()
         self.grids = [tuple(int(v) for v in g) for g in grids]
         self.n = len(self.grids)
@@ -278,6 +289,22 @@ class Batch:
         h = ctypes.c_void_p()
         _check(lib.gpufft_batch_create(ctypes.byref(h), self.n, dims, dd, self.dtype_code))
         self._h = h
+        if schedule == "auto":
+            _check(lib.gpufft_batch_autotune(h, _stream_handle(stream)))
+        elif schedule in ("persistent", "branches"):
+            self.set_schedule(schedule, branches)
+        else:
+            raise ValueError(f"unknown schedule {schedule!r}")
+
+    def set_schedule(self, schedule: str, branches: int = 4) -> None:
+        code = GPUFFT_BATCH_BRANCHES if schedule == "branches" else GPUFFT_BATCH_PERSISTENT
+        _check(load_library().gpufft_batch_set_schedule(self._h, code, int(branches)))
+
+    def schedule(self) -> tuple:
+        """("persistent" | "branches", number of branches)"""
+        s, b = ctypes.c_int(), ctypes.c_int()
+        _check(load_library().gpufft_batch_schedule(self._h, ctypes.byref(s), ctypes.byref(b)))
+        return ("branches" if s.value == GPUFFT_BATCH_BRANCHES else "persistent", b.value)
 
     def _ptrs(self, fields):
         if len(fields) != self.n:

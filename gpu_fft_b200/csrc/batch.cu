@@ -20,6 +20,15 @@
 // transform's own radix plan and twiddle tables, so one kernel serves any mix
 // of grids.  Scratch: the queue head, one counter per transform and an error
 // word, cleared by a memset node before every launch.
+//
+// Second schedule ("branches"): each transform runs its own plan's
+// specialised kernels, the transforms spread over a few concurrent streams
+// (largest first, each to the least loaded stream), forked from and joined
+// back into the caller's stream; exec_graph captures the fork/join into one
+// CUDA graph.  No item waits on another inside a kernel.  The batch
+// autotuner (gpufft_batch_autotune) tunes the transforms' plans and times
+// the persistent launch against 2, 4 and 8 branches on scratch fields, and
+// keeps the fastest.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -150,6 +159,12 @@ __global__ void __launch_bounds__(kThreads) batch_kernel(const BatchDesc *__rest
     }
 }
 
+constexpr int kMaxBranches = 8;
+
+static size_t field_bytes_of(const Plan &P) {
+    return (size_t)P.nx * P.ny * (P.nz / 2 + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16);
+}
+
 struct Batch {
     int n = 0;
     int dtype = 0;
@@ -168,11 +183,28 @@ struct Batch {
     cudaGraphExec_t gexec = nullptr;
     bool gready = false;
     std::vector<void *> uploaded;  // data pointers the device descriptors hold
+    // branches schedule
+    int schedule = GPUFFT_BATCH_PERSISTENT;
+    int nbranch = 4;
+    std::vector<int> branch_of;          // transform -> stream
+    std::vector<int> order;              // transforms, largest first
+    cudaStream_t bstream[kMaxBranches] = {};
+    cudaEvent_t fork = nullptr, join[kMaxBranches] = {};
+    cudaGraphExec_t gexec_br = nullptr;  // captured fork/join, for br_ptrs / br_nbranch
+    std::vector<void *> br_ptrs;
+    int br_nbranch = 0;
+    float tuned_ms = 0.f;                // graph time of the schedule the autotuner kept
 };
 
 static void batch_free(Batch *B) {
     if (!B) return;
     if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    if (B->gexec_br) cudaGraphExecDestroy(B->gexec_br);
+    for (int b = 0; b < kMaxBranches; ++b) {
+        if (B->bstream[b]) cudaStreamDestroy(B->bstream[b]);
+        if (B->join[b]) cudaEventDestroy(B->join[b]);
+    }
+    if (B->fork) cudaEventDestroy(B->fork);
     if (B->ddesc) cudaFree(B->ddesc);
     if (B->ditems) cudaFree(B->ditems);
     if (B->dscratch) cudaFree(B->dscratch);
@@ -227,6 +259,8 @@ static int batch_configure(Batch &B) {
     return GPUFFT_SUCCESS;
 }
 
+static void batch_assign(Batch &B, int nb);
+
 static int batch_create(Batch **out, int n, const int64_t *dims, const int *directions, int dtype) {
     if (!out) return set_error(GPUFFT_ERR_INVALID, "batch pointer is NULL");
     *out = nullptr;
@@ -253,6 +287,7 @@ static int batch_create(Batch **out, int n, const int64_t *dims, const int *dire
         batch_free(B);
         return rc;
     }
+    batch_assign(*B, B->nbranch);
     B->scratch_bytes = sizeof(BatchScratch) + sizeof(int) * (size_t)n;
     cudaError_t e = cudaMalloc(&B->ddesc, sizeof(BatchDesc) * (size_t)n);
     if (e == cudaSuccess) e = cudaMalloc(&B->ditems, sizeof(BatchItem) * std::max<size_t>(1, B->hitems.size()));
@@ -288,6 +323,59 @@ static int batch_upload(Batch &B, void *const *data, cudaStream_t s) {
     return GPUFFT_SUCCESS;
 }
 
+// Transform -> stream for `nb` branches: largest field first, each to the
+// stream with the fewest bytes so far.
+static void batch_assign(Batch &B, int nb) {
+    B.order.resize(B.n);
+    for (int t = 0; t < B.n; ++t) B.order[t] = t;
+    std::stable_sort(B.order.begin(), B.order.end(), [&](int a, int b) {
+        return field_bytes_of(*B.plans[a]) > field_bytes_of(*B.plans[b]);
+    });
+    std::vector<size_t> load(nb, 0);
+    B.branch_of.assign(B.n, 0);
+    for (int t : B.order) {
+        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        B.branch_of[t] = b;
+        load[b] += field_bytes_of(*B.plans[t]);
+    }
+    B.nbranch = nb;
+}
+
+static int batch_streams(Batch &B) {
+    if (!B.fork && cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming) != cudaSuccess)
+        return set_error(GPUFFT_ERR_CUDA, "batch fork event");
+    for (int b = 0; b < kMaxBranches; ++b) {
+        if (!B.bstream[b] && cudaStreamCreateWithFlags(&B.bstream[b], cudaStreamNonBlocking) != cudaSuccess)
+            return set_error(GPUFFT_ERR_CUDA, "batch stream");
+        if (!B.join[b] && cudaEventCreateWithFlags(&B.join[b], cudaEventDisableTiming) != cudaSuccess)
+            return set_error(GPUFFT_ERR_CUDA, "batch join event");
+    }
+    return GPUFFT_SUCCESS;
+}
+
+// Branches schedule: fork from s, every transform on its stream with its own
+// plan, join back into s (the joins are issued whatever happened, so a
+// capture of s always ends cleanly).
+static int branch_launch(Batch &B, void *const *data, cudaStream_t s) {
+    int rc = batch_streams(B);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    const int nb = B.nbranch;
+    cudaError_t e = cudaEventRecord(B.fork, s);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "batch fork: %s", cudaGetErrorString(e));
+    for (int b = 0; b < nb; ++b) cudaStreamWaitEvent(B.bstream[b], B.fork, 0);
+    for (int t : B.order) {
+        if (rc != GPUFFT_SUCCESS) break;
+        rc = plan_exec(B.plans[t], data[t], B.bstream[B.branch_of[t]], B.forward[t] != 0);
+    }
+    for (int b = 0; b < nb; ++b) {
+        cudaEventRecord(B.join[b], B.bstream[b]);
+        cudaStreamWaitEvent(s, B.join[b], 0);
+    }
+    e = cudaGetLastError();
+    if (rc == GPUFFT_SUCCESS && e != cudaSuccess) rc = set_error(GPUFFT_ERR_CUDA, "batch branches: %s", cudaGetErrorString(e));
+    return rc;
+}
+
 // clear the scratch, launch (the part a CUDA graph replays)
 static int batch_launch(Batch &B, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(B.dscratch, 0, B.scratch_bytes, s);
@@ -317,48 +405,198 @@ extern "C" int gpufft_batch_destroy(gpufft_batch batch) {
     return GPUFFT_SUCCESS;
 }
 
+static int check_ptrs(const Batch &B, void *const *data) {
+    if (!data) return set_error(GPUFFT_ERR_INVALID, "data array is NULL");
+    for (int t = 0; t < B.n; ++t) {
+        if (!data[t]) return set_error(GPUFFT_ERR_INVALID, "batch data pointer %d is NULL", t);
+        if (((uintptr_t)data[t]) % (B.dtype == GPUFFT_FLOAT ? 8 : 16) != 0)
+            return set_error(GPUFFT_ERR_INVALID, "batch data pointer %d is not aligned", t);
+    }
+    return GPUFFT_SUCCESS;
+}
+
+static int batch_exec(Batch &B, void *const *data, cudaStream_t s) {
+    int rc = check_ptrs(B, data);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    if (B.schedule == GPUFFT_BATCH_BRANCHES) return branch_launch(B, data, s);
+    rc = batch_upload(B, data, s);
+    return rc != GPUFFT_SUCCESS ? rc : batch_launch(B, s);
+}
+
+// Captures what `launch` issues on a private stream into an executable graph.
+template <class F>
+static int capture_graph(cudaGraphExec_t *out, F launch) {
+    cudaStream_t cs;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "capture stream: %s", cudaGetErrorString(e));
+    cudaGraph_t graph = nullptr;
+    int rc = GPUFFT_SUCCESS;
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) rc = launch(cs);
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess || e2 != cudaSuccess || rc != GPUFFT_SUCCESS) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc != GPUFFT_SUCCESS ? rc : set_error(GPUFFT_ERR_CUDA, "batch capture failed");
+    }
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return set_error(GPUFFT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    return GPUFFT_SUCCESS;
+}
+
+static int batch_exec_graph(Batch &B, void *const *data, cudaStream_t s) {
+    int rc = check_ptrs(B, data);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    if (B.schedule == GPUFFT_BATCH_BRANCHES) {
+        // the kernels' arguments hold the data pointers: captured again when they change
+        const bool same = B.gexec_br && B.br_nbranch == B.nbranch && B.br_ptrs.size() == (size_t)B.n &&
+                          std::equal(B.br_ptrs.begin(), B.br_ptrs.end(), data);
+        if (!same) {
+            if (B.gexec_br) cudaGraphExecDestroy(B.gexec_br);
+            B.gexec_br = nullptr;
+            rc = capture_graph(&B.gexec_br, [&](cudaStream_t cs) { return branch_launch(B, data, cs); });
+            if (rc != GPUFFT_SUCCESS) return rc;
+            B.br_ptrs.assign(data, data + B.n);
+            B.br_nbranch = B.nbranch;
+        }
+        const cudaError_t e = cudaGraphLaunch(B.gexec_br, s);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+    }
+    rc = batch_upload(B, data, s);
+    if (rc != GPUFFT_SUCCESS) return rc;
+    if (!B.gready) {
+        // captured once: the scratch memset and the persistent kernel; the
+        // descriptors it reads are refreshed on the stream by batch_upload
+        rc = capture_graph(&B.gexec, [&](cudaStream_t cs) { return batch_launch(B, cs); });
+        if (rc != GPUFFT_SUCCESS) return rc;
+        B.gready = true;
+    }
+    const cudaError_t e = cudaGraphLaunch(B.gexec, s);
+    return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+}
+
+// mean ms of `reps` graph replays of the current schedule on `data`
+static float time_schedule(Batch &B, void *const *data, cudaStream_t s, int reps) {
+    for (int w = 0; w < 2; ++w)
+        if (batch_exec_graph(B, data, s) != GPUFFT_SUCCESS) return 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    int rc = GPUFFT_SUCCESS;
+    for (int r = 0; r < reps && rc == GPUFFT_SUCCESS; ++r) rc = batch_exec_graph(B, data, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc == GPUFFT_SUCCESS ? ms / reps : 1e30f;
+}
+
+static int batch_autotune(Batch &B, cudaStream_t s) {
+    // scratch fields, one per transform, 256-byte aligned
+    std::vector<size_t> off(B.n);
+    size_t total = 0;
+    for (int t = 0; t < B.n; ++t) {
+        off[t] = total;
+        total += (field_bytes_of(*B.plans[t]) + 255) / 256 * 256;
+    }
+    char *buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, total);
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_OOM, "batch autotune scratch (%zu bytes): %s", total,
+                                           cudaGetErrorString(e));
+    cudaMemsetAsync(buf, 0, total, s);
+    std::vector<void *> ptrs(B.n);
+    for (int t = 0; t < B.n; ++t) ptrs[t] = buf + off[t];
+    // each distinct grid's plan tuned once, the others take its choice
+    int rc = GPUFFT_SUCCESS;
+    for (int t = 0; t < B.n && rc == GPUFFT_SUCCESS; ++t) {
+        const Plan &P = *B.plans[t];
+        int u = 0;
+        while (u < t && !(B.plans[u]->nx == P.nx && B.plans[u]->ny == P.ny && B.plans[u]->nz == P.nz)) ++u;
+        rc = u < t ? plan_adopt(B.plans[t], B.plans[u]) : plan_autotune(B.plans[t], ptrs[t], s);
+    }
+    // schedules: the persistent launch, then 2, 4 and 8 branches
+    int best_sched = GPUFFT_BATCH_PERSISTENT, best_nb = B.nbranch;
+    float best_ms = 1e30f;
+    if (rc == GPUFFT_SUCCESS) {
+        const int reps = total > (512u << 20) ? 3 : 8;
+        B.schedule = GPUFFT_BATCH_PERSISTENT;
+        best_ms = time_schedule(B, ptrs.data(), s, reps);
+        for (int nb : {2, 4, 8}) {
+            B.schedule = GPUFFT_BATCH_BRANCHES;
+            batch_assign(B, std::min(nb, B.n));
+            const float ms = time_schedule(B, ptrs.data(), s, reps);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_sched = GPUFFT_BATCH_BRANCHES;
+                best_nb = B.nbranch;
+            }
+        }
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(buf);
+    // graphs captured on the scratch pointers are of no further use
+    if (B.gexec_br) cudaGraphExecDestroy(B.gexec_br);
+    B.gexec_br = nullptr;
+    B.br_ptrs.clear();
+    B.uploaded.clear();
+    B.schedule = best_sched;
+    batch_assign(B, best_nb);
+    B.tuned_ms = best_ms;
+    return rc;
+}
+
 extern "C" int gpufft_batch_exec(gpufft_batch batch, void *const *data, void *stream) {
     Batch *B = reinterpret_cast<Batch *>(batch);
     if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
-    if (!data) return set_error(GPUFFT_ERR_INVALID, "data array is NULL");
-    const int rc = batch_upload(*B, data, (cudaStream_t)stream);
-    return rc != GPUFFT_SUCCESS ? rc : batch_launch(*B, (cudaStream_t)stream);
+    return batch_exec(*B, data, (cudaStream_t)stream);
 }
 
 extern "C" int gpufft_batch_exec_graph(gpufft_batch batch, void *const *data, void *stream) {
     Batch *B = reinterpret_cast<Batch *>(batch);
     if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
-    if (!data) return set_error(GPUFFT_ERR_INVALID, "data array is NULL");
-    cudaStream_t s = (cudaStream_t)stream;
-    int rc = batch_upload(*B, data, s);
-    if (rc != GPUFFT_SUCCESS) return rc;
-    if (!B->gready) {
-        // capture once: the scratch memset and the persistent kernel; the
-        // descriptors it reads are refreshed on the stream by batch_upload
-        cudaStream_t cs;
-        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "capture stream: %s", cudaGetErrorString(e));
-        cudaGraph_t graph = nullptr;
-        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) rc = batch_launch(*B, cs);
-        const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
-        cudaStreamDestroy(cs);
-        if (e != cudaSuccess || e2 != cudaSuccess || rc != GPUFFT_SUCCESS) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc != GPUFFT_SUCCESS ? rc : set_error(GPUFFT_ERR_CUDA, "batch capture failed");
-        }
-        e = cudaGraphInstantiate(&B->gexec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-        B->gready = true;
-    }
-    const cudaError_t e = cudaGraphLaunch(B->gexec, s);
-    return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+    return batch_exec_graph(*B, data, (cudaStream_t)stream);
+}
+
+extern "C" int gpufft_batch_set_schedule(gpufft_batch batch, int schedule, int branches) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    if (schedule != GPUFFT_BATCH_PERSISTENT && schedule != GPUFFT_BATCH_BRANCHES)
+        return set_error(GPUFFT_ERR_INVALID, "schedule %d is neither GPUFFT_BATCH_PERSISTENT nor _BRANCHES", schedule);
+    if (schedule == GPUFFT_BATCH_BRANCHES && (branches < 1 || branches > kMaxBranches))
+        return set_error(GPUFFT_ERR_INVALID, "branches must be 1..%d", kMaxBranches);
+    B->schedule = schedule;
+    if (schedule == GPUFFT_BATCH_BRANCHES) batch_assign(*B, std::min(branches, B->n));
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_batch_schedule(gpufft_batch batch, int *schedule, int *branches) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    if (schedule) *schedule = B->schedule;
+    if (branches) *branches = B->nbranch;
+    return GPUFFT_SUCCESS;
+}
+
+extern "C" int gpufft_batch_autotune(gpufft_batch batch, void *stream) {
+    Batch *B = reinterpret_cast<Batch *>(batch);
+    if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    return batch_autotune(*B, (cudaStream_t)stream);
 }
 
 extern "C" int gpufft_batch_status(gpufft_batch batch, void *stream) {
     Batch *B = reinterpret_cast<Batch *>(batch);
     if (!B) return set_error(GPUFFT_ERR_NOT_INIT, "no batch");
+    if (B->schedule == GPUFFT_BATCH_BRANCHES) {  // nothing waits inside a kernel
+        const cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "batch status: %s", cudaGetErrorString(e));
+    }
     int err = 0;
     cudaError_t e = cudaMemcpyAsync(&err, &B->dscratch->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);

@@ -687,6 +687,17 @@ int plan_create(Plan **out, int64_t nx, int64_t ny, int64_t nz, int dtype, int f
     return GPUFFT_SUCCESS;
 }
 
+int plan_adopt(Plan *P, const Plan *Q) {
+    if (!P || !Q) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    if (P->nx != Q->nx || P->ny != Q->ny || P->nz != Q->nz || P->dtype != Q->dtype || P->tc_split != Q->tc_split)
+        return set_error(GPUFFT_ERR_INVALID, "plan_adopt: the plans differ in grid or form");
+    if (Q->idx_a < 0 && Q->idx_b < 0) return GPUFFT_SUCCESS;  // generic kernels: nothing to copy
+    P->kfix = Q->kfix;
+    const int rc = setup_fast(*P, Q->idx_a, Q->idx_b);
+    if (rc == GPUFFT_SUCCESS) P->tuned = Q->tuned;
+    return rc;
+}
+
 int plan_destroy(Plan *P) {
     if (!P) return GPUFFT_SUCCESS;
     if (P->tw_dev) {

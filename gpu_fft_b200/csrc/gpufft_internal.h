@@ -52,6 +52,8 @@ int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forwa
 int plan_launches(const Plan *P);
 int plan_describe(const Plan *P, char *buf, int len);
 int plan_autotune(Plan *P, void *scratch, void *stream);
+// P takes Q's kernel choice (same grid, precision and form; Q tuned already)
+int plan_adopt(Plan *P, const Plan *Q);
 int wisdom_save(const char *path);
 int wisdom_load(const char *path);
 

@@ -176,6 +176,21 @@ int gpufft_batch_exec_graph(gpufft_batch batch, void *const *data, void *stream)
 int gpufft_batch_status(gpufft_batch batch, void *stream);
 /* Work items per launch. */
 int gpufft_batch_items(gpufft_batch batch);
+/* Schedules.  PERSISTENT (the default): the one persistent launch above.
+ * BRANCHES: each transform runs its own plan's specialised kernels, the
+ * transforms spread over `branches` (1..8) concurrent streams forked from
+ * and joined back into the caller's stream (largest field first, each to the
+ * least loaded stream); exec_graph captures the fork/join as one CUDA graph
+ * (captured again when the data pointers change).  Results are bitwise those
+ * of the transforms' own plans. */
+#define GPUFFT_BATCH_PERSISTENT 0
+#define GPUFFT_BATCH_BRANCHES 1
+int gpufft_batch_set_schedule(gpufft_batch batch, int schedule, int branches);
+int gpufft_batch_schedule(gpufft_batch batch, int *schedule, int *branches);
+/* Tunes every distinct grid's plan (gpufft_plan_autotune), then times the
+ * persistent launch and 2, 4 and 8 branches (graph replays on scratch
+ * fields it allocates and frees) and keeps the fastest schedule. */
+int gpufft_batch_autotune(gpufft_batch batch, void *stream);
 
 /* --------------------------------------------------------------------------
  * Precision form (no counterpart in the reference, which is FP32/FP64 only,

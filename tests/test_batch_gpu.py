@@ -102,3 +102,68 @@ def test_spectral_step_batch_3_c2r_6_r2c(cuda):
     batch.status()
     for a, b in zip(fields, want):
         assert _rel(a, b) < TOL
+
+
+@pytest.mark.parametrize("branches", [1, 3, 8])
+def test_branches_schedule_is_bitwise_the_transforms_own_plans(cuda, branches):
+    """The branches schedule runs each transform's own plan on one of several
+    forked streams: direct and graph-replayed (with new pointers) results are
+    bitwise those of the plans run one by one."""
+    import torch
+    import gpu_fft_b200 as g
+
+    dirs = ["r2c", "c2r", "r2c", "r2c", "c2r", "r2c", "c2r", "c2r"]
+    batch = g.Batch(GRIDS, dirs, "float", schedule="branches", branches=branches)
+    assert batch.schedule() == ("branches", min(branches, len(GRIDS)))
+    for rep, graph in enumerate((False, True, True)):
+        fields = [_field(gr, 50 * rep + i, torch.float32) for i, gr in enumerate(GRIDS)]
+        want = [f.clone() for f in fields]
+        for f, gr, d in zip(want, GRIDS, dirs):
+            p = g.Plan(*gr)
+            (p.r2c if d == "r2c" else p.c2r)(f)
+        batch.exec(fields, graph=graph)
+        batch.status()
+        for a, b, gr in zip(fields, want, GRIDS):
+            assert torch.equal(a, b), (gr, rep)
+
+
+def test_batch_autotune_picks_a_schedule_that_matches_the_plans(cuda):
+    import torch
+    import gpu_fft_b200 as g
+
+    grids = [(64, 64, 64), (128, 128, 128), (96, 96, 96), (64, 64, 64), (48, 40, 30)]
+    dirs = ["r2c", "r2c", "c2r", "c2r", "r2c"]
+    batch = g.Batch(grids, dirs, "float", schedule="auto")
+    sched, nb = batch.schedule()
+    assert sched in ("persistent", "branches") and 1 <= nb <= 8
+    fields = [_field(gr, 300 + i, torch.float32) for i, gr in enumerate(grids)]
+    want = [f.clone() for f in fields]
+    for f, gr, d in zip(want, grids, dirs):
+        p = g.Plan(*gr)
+        (p.r2c if d == "r2c" else p.c2r)(f)
+    batch.exec(fields, graph=True)
+    batch.status()
+    for a, b in zip(fields, want):
+        assert _rel(a, b) < TOL
+    # the other schedule on the same batch agrees too
+    batch.set_schedule("persistent" if sched == "branches" else "branches", 2)
+    again = [_field(gr, 300 + i, torch.float32) for i, gr in enumerate(grids)]
+    batch.exec(again, graph=True)
+    batch.status()
+    for a, b in zip(again, want):
+        assert _rel(a, b) < TOL
+
+
+def test_batch_schedule_arguments_are_checked(cuda):
+    import ctypes
+
+    import gpu_fft_b200 as g
+
+    batch = g.Batch([(8, 8, 8)], ["r2c"], "float")
+    lib = g.load_library()
+    assert lib.gpufft_batch_set_schedule(batch._h, 7, 2) == 1
+    assert lib.gpufft_batch_set_schedule(batch._h, g.GPUFFT_BATCH_BRANCHES, 0) == 1
+    assert lib.gpufft_batch_set_schedule(batch._h, g.GPUFFT_BATCH_BRANCHES, 9) == 1
+    s, b = ctypes.c_int(), ctypes.c_int()
+    assert lib.gpufft_batch_schedule(batch._h, ctypes.byref(s), ctypes.byref(b)) == 0
+    assert s.value == g.GPUFFT_BATCH_PERSISTENT
