@@ -18,6 +18,12 @@
      (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB>,  \
      (const void *)pass_b_pipe<T, NX, W, NT, true, V, MINB, true>,                                                  \
      (const void *)pass_b_pipe<T, NX, W, NT, false, V, MINB, true>}
+// one tile buffer, refilled by cp.async while the last stage computes
+#define Q_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
+    {2, DT, NX, W, NT, V, (size_t)(((NX + 1) / 2 * 2) + NX * W) * sizeof(cx_t<T>),                              \
+     (const void *)pass_b_pipe1<T, NX, W, NT, true, V, MINB>, (const void *)pass_b_pipe1<T, NX, W, NT, false, V, MINB>, \
+     (const void *)pass_b_pipe1<T, NX, W, NT, true, V, MINB, true>,                                                 \
+     (const void *)pass_b_pipe1<T, NX, W, NT, false, V, MINB, true>}
 #define B_ENTRY(T, DT, NX, W, NT, V, MINB)                                                                    \
     {0, DT, NX, W, NT, V, (size_t)(NX + NX * W) * sizeof(cx_t<T>), (const void *)pass_b_fast<T, NX, W, NT, true, V, MINB>, \
      (const void *)pass_b_fast<T, NX, W, NT, false, V, MINB>,                                                       \

@@ -36,8 +36,10 @@ const VariantB kVariantsB_f32[] = {
     P_ENTRY(float, 0, 512, 8, 512, 0, 2),
     B_ENTRY(float, 0, 512, 16, 256, 1, 2),
     B_ENTRY(float, 0, 512, 16, 256, 0, 3),
-    // 128-byte tile rows matter more than double buffering at Nx = 1024:
-    // 2.38 ms per launch at 1024^3 against 3.54 ms for 8-column tiles
+    // 128-byte tile rows matter more than double buffering at Nx = 1024
+    // (2.36 ms per launch at 1024^3 against 3.57 ms for 8-column tiles); the
+    // one 128 KB tile buffer refilled during the last stage: 1.83 ms
+    Q_ENTRY(float, 0, 1024, 16, 512, 0, 1),
     B_ENTRY(float, 0, 1024, 16, 512, 0, 1),
     B_ENTRY(float, 0, 1024, 16, 1024, 0, 1),
     B_ENTRY(float, 0, 1024, 8, 256, 0, 2),
@@ -52,11 +54,17 @@ const VariantB kVariantsB_f32[] = {
     B_ENTRY(float, 0, 128, 16, 256, 0, 2),
     B_ENTRY(float, 0, 96, 16, 256, 0, 2),
     B_ENTRY(float, 0, 64, 16, 256, 0, 2),
+    // one refilled tile buffer (measured at 512^3: 0.219 / 0.253 ms against
+    // 0.207 for the double-buffered kernel; at 1024^3 1.88 ms with 1024 threads)
+    Q_ENTRY(float, 0, 1024, 16, 1024, 0, 1),
+    Q_ENTRY(float, 0, 512, 16, 256, 1, 2),
+    Q_ENTRY(float, 0, 512, 16, 512, 1, 1),
     // tensor-core radix-16 stages (v = 2): only plans made with
     // GPUFFT_PLAN_TC_SPLIT use these, and they use nothing else
     P_ENTRY(float, 0, 512, 16, 512, 2, 1),
     P_ENTRY(float, 0, 512, 16, 256, 2, 2),
     B_ENTRY(float, 0, 512, 16, 256, 2, 2),
+    Q_ENTRY(float, 0, 1024, 16, 512, 2, 1),
     B_ENTRY(float, 0, 1024, 16, 512, 2, 1),
 };
 const int kNumVariantsB_f32 = sizeof(kVariantsB_f32) / sizeof(kVariantsB_f32[0]);

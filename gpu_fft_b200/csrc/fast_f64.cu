@@ -22,8 +22,10 @@ const VariantB kVariantsB_f64[] = {
     P_ENTRY(double, 1, 512, 4, 256, 0, 2),
     B_ENTRY(double, 1, 512, 8, 256, 0, 2),
     B_ENTRY(double, 1, 512, 4, 256, 0, 2),
+    Q_ENTRY(double, 1, 512, 8, 256, 0, 2),
     B_ENTRY(double, 1, 128, 8, 256, 0, 2),
     // 1024 (8 x 16-byte complex = 128-byte tile rows), 384, 256
+    Q_ENTRY(double, 1, 1024, 8, 512, 0, 1),
     B_ENTRY(double, 1, 1024, 8, 512, 0, 1),
     B_ENTRY(double, 1, 1024, 4, 256, 0, 1),
     P_ENTRY(double, 1, 384, 8, 256, 0, 1),

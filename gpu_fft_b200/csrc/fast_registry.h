@@ -23,7 +23,8 @@ struct VariantA {
 };
 
 struct VariantB {
-    int kind;  // 0: tiles loaded by the first FFT stage; 1: tiles double-buffered by cp.async
+    int kind;  // 0: tiles loaded by the first FFT stage; 1: tiles double-buffered by cp.async;
+               // 2: one tile buffer refilled by cp.async during the last stage
     int dtype;
     int nx;
     int w, nt, v;

@@ -170,6 +170,9 @@ struct TileLayout {
 // stage writes, the shared tile itself (natural order).
 struct FromSmem {};
 struct ToSmem {};
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
 
 template <typename T, int N, int W, int NT, bool FWD, int LAYOUT, int VARIANT = 0, int SCOPE = BLOCK>
 struct TileFFT {
@@ -366,18 +369,21 @@ struct TileFFT {
         *reinterpret_cast<float4 *>(sm + idx) = make_float4(a.x, a.y, b.x, b.y);
     }
 
-    template <int S, class Src, class Dst>
-    static __device__ __forceinline__ void stage(Src &src, Dst &dst, V *sm, const V *tw) {
+    template <int S, class Src, class Dst, class Hook>
+    static __device__ __forceinline__ void stage(Src &src, Dst &dst, V *sm, const V *tw, Hook &hook) {
         if constexpr (kTcStage && F.r[S] == 16 && S < NS - 1) {
             stage_tc16<S>(src, dst, sm, tw);
             return;
         } else {
-            stage_scalar<S>(src, dst, sm, tw);
+            stage_scalar<S>(src, dst, sm, tw, hook);
         }
     }
 
-    template <int S, class Src, class Dst>
-    static __device__ __forceinline__ void stage_scalar(Src &src, Dst &dst, V *sm, const V *tw) {
+    // Hook: called by every thread once the last stage has read the whole
+    // tile from shared memory (after a barrier) when the last stage writes
+    // global memory -- the tile buffer is free from then on.  NoHook: none.
+    template <int S, class Src, class Dst, class Hook>
+    static __device__ __forceinline__ void stage_scalar(Src &src, Dst &dst, V *sm, const V *tw, Hook &hook) {
         constexpr int R = F.r[S];
         constexpr int p = fac_prod(F, S);
         constexpr int nb = N / R;
@@ -417,6 +423,10 @@ struct TileFFT {
             }
         }
         if (dst_smem) sync();  // every reader of the tile is done before it is overwritten
+        if constexpr (last && !dst_smem && src_smem && !std::is_same<Hook, NoHook>::value) {
+            sync();
+            hook();
+        }
         // In the COLS layout a thread's butterflies are NT/W apart in i; when
         // that is a multiple of p they share k = i mod p, so their twiddles
         // are read from shared memory once.
@@ -463,11 +473,11 @@ struct TileFFT {
         }
     }
 
-    template <int S, class Src, class Dst>
-    static __device__ __forceinline__ void stages(Src &src, Dst &dst, V *sm, const V *tw) {
+    template <int S, class Src, class Dst, class Hook>
+    static __device__ __forceinline__ void stages(Src &src, Dst &dst, V *sm, const V *tw, Hook &hook) {
         if constexpr (S < NS) {
-            stage<S>(src, dst, sm, tw);
-            stages<S + 1>(src, dst, sm, tw);
+            stage<S>(src, dst, sm, tw, hook);
+            stages<S + 1>(src, dst, sm, tw, hook);
         }
     }
 
@@ -476,6 +486,11 @@ struct TileFFT {
     // complete only after the caller's next __syncthreads().
     template <class Src, class Dst>
     static __device__ __forceinline__ void run(Src &src, Dst &dst, V *sm, const V *tw) {
+        NoHook none;
+        run(src, dst, sm, tw, none);
+    }
+    template <class Src, class Dst, class Hook>
+    static __device__ __forceinline__ void run(Src &src, Dst &dst, V *sm, const V *tw, Hook &hook) {
         if constexpr (NS == 0) {
             // length 1: identity (copy)
             if constexpr (std::is_same<Src, FromSmem>::value) sync();
@@ -492,7 +507,7 @@ struct TileFFT {
                     dst(0, q, x);
             }
         } else {
-            stages<0>(src, dst, sm, tw);
+            stages<0>(src, dst, sm, tw, hook);
         }
     }
 };
@@ -612,6 +627,67 @@ __global__ void __launch_bounds__(NT, MINB) pass_b_pipe(PassBParams P) {
         FromSmem fs;
         FFT::run(fs, dst, cur, tw);
         __syncthreads();  // the tile is free for the copy issued next iteration
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pass B with ONE tile buffer refilled early: the next tile's cp.async copies
+// are issued as soon as the last FFT stage has read the current tile from
+// shared memory, so they stream in while that stage computes and writes its
+// results to global memory.  For tiles too large to double-buffer
+// (Nx = 1024 with 16-column tiles: 128 KB).  Same alignment rules as
+// pass_b_pipe.
+// ---------------------------------------------------------------------------
+template <typename T, int NX, int W, int NT, bool FWD, int VARIANT, int MINB, bool EPI = false>
+__global__ void __launch_bounds__(NT, MINB) pass_b_pipe1(PassBParams P) {
+    using V = cx_t<T>;
+    using FFT = TileFFT<T, NX, W, NT, FWD, COLS, VARIANT, BLOCK>;
+    constexpr int PER16 = 16 / (int)sizeof(V);
+    constexpr int CH = W / PER16;
+    static_assert(W % PER16 == 0, "tile rows must be whole 16-byte chunks");
+    static_assert(FFT::NS >= 2, "the first stage must read the tile from shared memory");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *buf = tw + ((NX + PER16 - 1) / PER16) * PER16;
+    for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
+    const V *base = reinterpret_cast<const V *>(P.data);
+    V *obase = reinterpret_cast<V *>(P.data);
+    const long long ncols = P.ncols;
+    auto prefetch = [&](long long t) {
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        for (int q = threadIdx.x; q < NX * CH; q += NT) {
+            const int n = q / CH, ch = q % CH;
+            const int w = ch * PER16;
+            const int valid = max(0, min(PER16, wv - w));
+            const V *src = base + (long long)n * ncols + c0 + (valid > 0 ? w : 0);
+            cp_async16(buf + FFT::L::idx(n, w), src, valid * (int)sizeof(V));
+        }
+        cp_async_commit();
+    };
+    long long t = blockIdx.x;
+    if (t < P.ntiles) prefetch(t);
+    for (; t < P.ntiles; t += gridDim.x) {
+        cp_async_wait<0>();
+        // (the first stage begins with a block barrier: every thread's copies
+        // have landed before any thread reads the tile)
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        V *g = obase + c0;
+        auto dst = [&](int n, int w, V v) {
+            if (w < wv) {
+                if constexpr (EPI)
+                    st_g(g + (long long)n * ncols + w, pass_b_epilogue(P, v, n, c0 + w));
+                else
+                    st_g(g + (long long)n * ncols + w, v);
+            }
+        };
+        const long long tn = t + gridDim.x;
+        auto refill = [&]() {
+            if (tn < P.ntiles) prefetch(tn);
+        };
+        FromSmem fs;
+        FFT::run(fs, dst, buf, tw, refill);
     }
 }
 

@@ -244,7 +244,7 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
 static bool b_eligible(const Plan &P, const fast::VariantB &v) {
     const int m = (int)(P.nz / 2);
     const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
-    return v.nx == (int)P.nx && (v.kind != 1 || rows16) && ((v.v == 2) == P.tc_split);
+    return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v == 2) == P.tc_split);
 }
 
 // Picks the specialised kernels for this plan's shape (first registry entry,
@@ -772,7 +772,7 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd, do
     prm.scale = scale;
     prm.dealias = dealias;
     prm.epi = (scale != 1.0 || dealias) ? 1 : 0;
-    if (P.fb && !(P.fb->kind == 1 && ((uintptr_t)data) % 16 != 0)) {
+    if (P.fb && !(P.fb->kind != 0 && ((uintptr_t)data) % 16 != 0)) {
         prm.wx = P.fb->w;
         prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
         void *args[] = {&prm};
