@@ -9,6 +9,11 @@
     {0, 0, DT, NY, M, RW, WY, NT, VY, VZ, PassAShape<T, NY, M, RW, WY, NT, VY, VZ>::smem_bytes(),              \
      (const void *)pass_a_fast<T, NY, M, RW, WY, NT, true, VY, VZ, MINB>,                                     \
      (const void *)pass_a_fast<T, NY, M, RW, WY, NT, false, VY, VZ, MINB>}
+// Pass A with the column tiles copied ahead by cp.async (CP = 1)
+#define AC_ENTRY(T, DT, NY, M, RW, WY, NT, VY, VZ, MINB)                                                     \
+    {0, 0, DT, NY, M, RW, WY, NT, VY, VZ, PassAShape<T, NY, M, RW, WY, NT, VY, VZ>::smem_bytes(),              \
+     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, true, VY, VZ, MINB, 1>,                                  \
+     (const void *)pass_a_fast<T, NY, M, RW, WY, NT, false, VY, VZ, MINB, 1>}
 #define D_ENTRY(T, DT, NY, M, RW, WY, NT, K, VY, VZ, MINB)                                                   \
     {1, K, DT, NY, M, RW, WY, NT, VY, VZ, PassADsmemShape<T, NY, M, RW, WY, NT, K, VY, VZ>::smem_bytes(),        \
      (const void *)pass_a_dsmem<T, NY, M, RW, WY, NT, K, true, VY, VZ, MINB>,                                    \

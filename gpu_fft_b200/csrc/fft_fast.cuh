@@ -566,6 +566,17 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// one complex element (8 or 16 bytes, both addresses aligned to its size);
+// zero-filled when `valid` is false
+template <typename V>
+__device__ __forceinline__ void cp_async_elem(V *smem, const V *gmem, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? (int)sizeof(V) : 0;
+    if constexpr (sizeof(V) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -721,7 +732,12 @@ __device__ __forceinline__ void cluster_wait() {
 // (rows [crank*NY/K, ...), column tiles crank, crank+K, ...), for planes
 // first_plane, first_plane + plane_step, ...  The kernel below runs it over
 // the grid; the batched form runs it for one whole plane (K = 1).
-template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ>
+// CP = 1: column tiles after the first are copied into the tile buffer by
+// cp.async, the next one issued as soon as the last FFT stage of the current
+// one has read the buffer (TileFFT::run's hook), so its loads overlap that
+// stage's arithmetic and stores.  Column tile 0 (the packed bins 0 and Nz/2)
+// keeps its own path.
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int CP = 0>
 __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned char *smem_raw, const int crank,
                                                 const int K, const int first_plane, const int plane_step) {
     using V = cx_t<T>;
@@ -752,7 +768,20 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
     const T hf = (T)0.5;
 
     // ---------------- y columns of plane g (whole CTA) ----------------
+    // CP: copies of column tile t (t >= 1) of plane g into the tile buffer
+    auto prefetch_cols = [&](V *g, int t) {
+        const int c0 = t * WY;
+        const int wv = min(WY, M - c0);
+        for (int q = threadIdx.x; q < NY * WY; q += NT) {
+            const int n = q / WY, w = q % WY;
+            cp_async_elem(tile + ColL::idx(n, w), g + (long long)n * NH + c0 + (w < wv ? w : 0), w < wv);
+        }
+        cp_async_commit();
+    };
     auto cols = [&](V *g) {
+        if constexpr (CP) {
+            if (crank != 0 && crank < ntiles_y) prefetch_cols(g, crank);
+        }
         for (int t = crank; t < ntiles_y; t += K) {
             const int c0 = t * WY;
             const int wv = min(WY, M - c0);
@@ -763,7 +792,16 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
             auto dst = [&](int n, int w, V v) {
                 if (w < wv) st_g(gc + (long long)n * NH + w, v);
             };
-            if (c0 != 0) {
+            if (CP && c0 != 0) {
+                cp_async_wait<0>();
+                // (the first stage begins with a block barrier)
+                const int tn = t + K;
+                auto refill = [&]() {
+                    if (tn < ntiles_y) prefetch_cols(g, tn);
+                };
+                FromSmem fs;
+                ColFFT::run(fs, dst, tile, sty, refill);
+            } else if (c0 != 0) {
                 ColFFT::run(src, dst, tile, sty);
             } else if (FWD) {
                 // column 0 carries (bin 0) + i (bin m); split after the FFT
@@ -798,6 +836,12 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
                 }
                 __syncthreads();
                 ColFFT::run(src, dst, tile, sty);
+            }
+            if constexpr (CP) {
+                if (c0 == 0 && t + K < ntiles_y) {
+                    __syncthreads();  // tile 0's last reads of the buffer are done
+                    prefetch_cols(g, t + K);
+                }
             }
         }
     };
@@ -915,12 +959,12 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
     }
 }
 
-template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB>
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB, int CP = 0>
 __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.K;
-    pass_a_fast_run<T, NY, M, RW, WY, NT, FWD, VY, VZ>(P, smem_raw, (int)blockIdx.x % K, K, (int)blockIdx.x / K,
-                                                       (int)gridDim.x / K);
+    pass_a_fast_run<T, NY, M, RW, WY, NT, FWD, VY, VZ, CP>(P, smem_raw, (int)blockIdx.x % K, K,
+                                                           (int)blockIdx.x / K, (int)gridDim.x / K);
 }
 
 // ---------------------------------------------------------------------------
