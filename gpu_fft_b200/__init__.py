@@ -33,7 +33,8 @@ EXPORTS = (
     "gpufft_exec_noalloc",
     "gpufft_batch_create", "gpufft_batch_destroy", "gpufft_batch_exec", "gpufft_batch_exec_graph",
     "gpufft_batch_status", "gpufft_batch_items", "gpufft_batch_set_schedule", "gpufft_batch_schedule",
-    "gpufft_batch_autotune",
+    "gpufft_batch_autotune", "gpufft_hostpipe_create", "gpufft_hostpipe_submit", "gpufft_hostpipe_join",
+    "gpufft_hostpipe_destroy",
     "gpufft_plan16_create", "gpufft_plan16_destroy", "gpufft_plan16_scale_count", "gpufft_exec16_r2c",
     "gpufft_exec16_c2r", "gpufft_exec16_pass", "gpufft_quantize16", "gpufft_dequantize16",
     "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
@@ -107,6 +108,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_batch_set_schedule.argtypes = [vp, ci, ci]
     lib.gpufft_batch_schedule.argtypes = [vp, ctypes.POINTER(ci), ctypes.POINTER(ci)]
     lib.gpufft_batch_autotune.argtypes = [vp, vp]
+    lib.gpufft_hostpipe_create.argtypes = [ctypes.POINTER(vp), vp, ci]
+    lib.gpufft_hostpipe_submit.argtypes = [vp, vp, vp, ci, vp]
+    lib.gpufft_hostpipe_join.argtypes = [vp, vp]
+    lib.gpufft_hostpipe_destroy.argtypes = [vp]
     lib.gpufft_plan16_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci]
     lib.gpufft_plan16_destroy.argtypes = [vp]
     lib.gpufft_plan16_scale_count.argtypes = [vp]
@@ -254,6 +259,49 @@ class Plan:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().gpufft_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostPipe:
+    """Transforms of fields in (pinned) host memory, pipelined over `depth`
+    device fields so that consecutive fields' copies in and out overlap
+    (gpufft_hostpipe_*).  submit() is stream-ordered and returns at once;
+    join() makes the stream wait for every submission.  The plan must
+    outlive the pipe."""
+
+    OPS = {"c2r": 0, "r2c": 1, "roundtrip": 2}
+
+    def __init__(self, plan: "Plan", depth: int = 3):
+        h = ctypes.c_void_p()
+        _check(load_library().gpufft_hostpipe_create(ctypes.byref(h), plan.handle, int(depth)))
+        self._h = h
+        self.plan = plan
+        self.bytes = plan.nx * plan.ny * nh_of(plan.nz) * (8 if plan.dtype_code == GPUFFT_FLOAT else 16)
+
+    def _host_ptr(self, t) -> int:
+        if t.is_cuda or not t.is_contiguous() or t.numel() * t.element_size() < self.bytes:
+            raise ValueError(f"host buffers must be contiguous CPU tensors of at least {self.bytes} bytes")
+        return t.data_ptr()
+
+    def submit(self, host_in, host_out, op: str = "roundtrip", stream=None) -> None:
+        _check(load_library().gpufft_hostpipe_submit(self._h, self._host_ptr(host_in), self._host_ptr(host_out),
+                                                      self.OPS[op], _stream_handle(stream)))
+
+    def submit_ptr(self, host_in: int, host_out: int, op: int, stream: int) -> None:
+        _check(load_library().gpufft_hostpipe_submit(self._h, host_in, host_out, op, stream))
+
+    def join(self, stream=None) -> None:
+        _check(load_library().gpufft_hostpipe_join(self._h, _stream_handle(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load_library().gpufft_hostpipe_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

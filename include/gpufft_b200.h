@@ -193,6 +193,28 @@ int gpufft_batch_schedule(gpufft_batch batch, int *schedule, int *branches);
 int gpufft_batch_autotune(gpufft_batch batch, void *stream);
 
 /* --------------------------------------------------------------------------
+ * Fields in host memory (no counterpart in the reference, whose transforms
+ * take device fields, FFT_R2C.cu:41-70): a pipe owns `depth` (1..8) device
+ * fields of `plan`'s size and three streams (copy-in, compute, copy-out).
+ * Each submission copies host_in to a free device field, runs the op
+ * (R2C, C2R, or R2C then C2R) and copies the result to host_out, stream-
+ * ordered after `stream` at the time of the call; the copy-in of the next
+ * submissions overlaps this one's compute and copy-out (PCIe carries both
+ * directions at once).  gpufft_hostpipe_join makes `stream` wait for every
+ * submission so far.  Host buffers of gpufft_field_bytes() bytes, pinned for
+ * the copies to overlap, untouched until the join.  `plan` must outlive the
+ * pipe.
+ * ------------------------------------------------------------------------ */
+#define GPUFFT_PIPE_C2R 0
+#define GPUFFT_PIPE_R2C 1
+#define GPUFFT_PIPE_ROUNDTRIP 2
+typedef struct gpufft_hostpipe_s *gpufft_hostpipe;
+int gpufft_hostpipe_create(gpufft_hostpipe *pipe, gpufft_plan plan, int depth);
+int gpufft_hostpipe_submit(gpufft_hostpipe pipe, const void *host_in, void *host_out, int op, void *stream);
+int gpufft_hostpipe_join(gpufft_hostpipe pipe, void *stream);
+int gpufft_hostpipe_destroy(gpufft_hostpipe pipe);
+
+/* --------------------------------------------------------------------------
  * Precision form (no counterpart in the reference, which is FP32/FP64 only,
  * GPU_FFT.h:112-120): the in-place field is stored in 16 bits — format 0 =
  * BF16, 1 = FP16 — half the bytes of the FP32 form, with one FP32 scale per
