@@ -12,6 +12,10 @@ const VariantA kVariantsA_f64[] = {
     // 1024x512x256: planes of 512 x 129
     A_ENTRY(double, 1, 512, 128, 2, 8, 256, 0, 0, 1),
     A_ENTRY(double, 1, 512, 128, 2, 4, 256, 0, 0, 1),
+    // 384x360x480 planes: spills about 800 bytes at 255 registers and is
+    // still faster than the generic kernels (0.79 / 0.90 ms per launch
+    // against 0.96 / 0.96)
+    A_ENTRY(double, 1, 360, 240, 2, 8, 256, 0, 0, 1),
     // 128^3 (the 256^2 plane spills even at 255 registers: generic)
     A_ENTRY(double, 1, 128, 64, 4, 8, 256, 0, 0, 1),
 };

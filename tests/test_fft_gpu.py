@@ -372,7 +372,8 @@ def test_autotune_keeps_results_identical_and_records_wisdom(oracle, cuda, tmp_p
                                      ((16, 1024, 1024), "float"), ((54, 54, 54), "float"), ((72, 72, 72), "float"),
                                      ((288, 288, 288), "float"), ((486, 486, 486), "float"),
                                      ((1024, 512, 256), "double"), ((128, 128, 128), "double"),
-                                     ((384, 64, 64), "double"), ((256, 64, 64), "double")], ids=str)
+                                     ((384, 64, 64), "double"), ((256, 64, 64), "double"),
+                                     ((384, 360, 480), "float"), ((384, 360, 480), "double")], ids=str)
 def test_every_compiled_candidate_matches_generic(cuda, grid, dt, monkeypatch):
     """The autotuner picks on speed alone, so every registered kernel candidate
     of both passes must compute the same transform as the generic kernels."""
