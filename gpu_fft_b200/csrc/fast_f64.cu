@@ -10,6 +10,9 @@ const VariantA kVariantsA_f64[] = {
     A_ENTRY(double, 1, 512, 256, 2, 8, 256, 0, 0, 2),
     A_ENTRY(double, 1, 512, 256, 2, 4, 256, 0, 0, 2),
     // 1024x512x256: planes of 512 x 129
+    // four rows per warp at 128 registers: 1.04 / 0.97 ms per launch on
+    // 2-CTA clusters against 1.03 / 1.08 for two rows
+    A_ENTRY(double, 1, 512, 128, 4, 8, 256, 0, 0, 2),
     A_ENTRY(double, 1, 512, 128, 2, 8, 256, 0, 0, 1),
     A_ENTRY(double, 1, 512, 128, 2, 4, 256, 0, 0, 1),
     // 384x360x480 planes: spills about 800 bytes at 255 registers and is
