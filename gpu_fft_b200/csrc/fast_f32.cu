@@ -21,9 +21,6 @@ const VariantA kVariantsA_f32[] = {
     // plane held in the cluster's shared memory: correct, measured slower at 512^3
     // (one 180 KB CTA per SM leaves 28 SMs idle); kept as an autotuning candidate
     D_ENTRY(float, 0, 512, 256, 2, 8, 512, 8, 0, 0, 1),
-    // four rows per warp: 0.460 / 0.436 ms per launch at 512^3 (K = 4)
-    // against 0.463 / 0.443 for two
-    A_ENTRY(float, 0, 512, 256, 4, 16, 256, 0, 0, 2),
     A_ENTRY(float, 0, 1024, 512, 1, 8, 256, 0, 0, 2),
     A_ENTRY(float, 0, 1024, 512, 1, 16, 512, 0, 0, 1),
     // 384x360x480 planes: two rows per warp and 16-column tiles at two CTAs
