@@ -203,25 +203,39 @@ static int exchange_nccl(const DistPlan &D, const void *from, void *to, cudaStre
     return GPUFFT_SUCCESS;
 }
 
+// Pass A with its y columns in the exchange layout (the send buffer): the
+// pack (forward) or unpack (inverse) copy folds into Pass A's own loads and
+// stores.  Plans whose Pass A runs the generic kernels pack and unpack.
+static bool fused_xch(const DistPlan &D) { return plan_has_xch(D.pa); }
+
+static int pass_a_xch(const DistPlan &D, void *data, cudaStream_t s, bool fwd) {
+    return plan_exec_pass_a_xch(D.pa, data, D.sendbuf, (int)D.nyl, (long long)(D.chunk / D.cs), s, fwd);
+}
+
 int dist_exec(DistPlan *D, void *data, cudaStream_t s, bool fwd) {
     if (!D) return set_error(GPUFFT_ERR_NOT_INIT, "no distributed plan");
     if (D->local) return set_error(GPUFFT_ERR_INVALID, "a plan of an in-process group runs through gpufft_dgroup_exec");
     if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
     int rc;
+    const bool fused = D->comm && fused_xch(*D);
     if (fwd) {
-        rc = plan_exec_pass(D->pa, data, s, 0, true);
-        if (D->comm) {
-            if (rc == GPUFFT_SUCCESS) rc = pack(*D, data, s);
-            if (rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, D->sendbuf, data, s);
+        if (fused) {
+            rc = pass_a_xch(*D, data, s, true);
+        } else {
+            rc = plan_exec_pass(D->pa, data, s, 0, true);
+            if (D->comm && rc == GPUFFT_SUCCESS) rc = pack(*D, data, s);
         }
+        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, D->sendbuf, data, s);
         if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D->pb, data, s, 1, true);
     } else {
         rc = plan_exec_pass(D->pb, data, s, 1, false);
-        if (D->comm) {
-            if (rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, data, D->sendbuf, s);
-            if (rc == GPUFFT_SUCCESS) rc = unpack(*D, data, s);
+        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, data, D->sendbuf, s);
+        if (fused) {
+            if (rc == GPUFFT_SUCCESS) rc = pass_a_xch(*D, data, s, false);
+        } else {
+            if (D->comm && rc == GPUFFT_SUCCESS) rc = unpack(*D, data, s);
+            if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D->pa, data, s, 0, false);
         }
-        if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D->pa, data, s, 0, false);
     }
     return rc;
 }
@@ -364,10 +378,15 @@ extern "C" int gpufft_dgroup_exec(gpufft_dplan *plans, void **data, int procs, i
         return GPUFFT_SUCCESS;
     };
     int rc = GPUFFT_SUCCESS;
+    const bool fused = procs > 1 && fused_xch(*D[0]);
     if (forward) {
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) {
-            rc = plan_exec_pass(D[r]->pa, data[r], s, 0, true);
-            if (rc == GPUFFT_SUCCESS && procs > 1) rc = pack(*D[r], data[r], s);
+            if (fused) {
+                rc = pass_a_xch(*D[r], data[r], s, true);
+            } else {
+                rc = plan_exec_pass(D[r]->pa, data[r], s, 0, true);
+                if (rc == GPUFFT_SUCCESS && procs > 1) rc = pack(*D[r], data[r], s);
+            }
         }
         if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange(true);
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) rc = plan_exec_pass(D[r]->pb, data[r], s, 1, true);
@@ -375,8 +394,12 @@ extern "C" int gpufft_dgroup_exec(gpufft_dplan *plans, void **data, int procs, i
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) rc = plan_exec_pass(D[r]->pb, data[r], s, 1, false);
         if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange(false);
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) {
-            if (procs > 1) rc = unpack(*D[r], data[r], s);
-            if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D[r]->pa, data[r], s, 0, false);
+            if (fused) {
+                rc = pass_a_xch(*D[r], data[r], s, false);
+            } else {
+                if (procs > 1) rc = unpack(*D[r], data[r], s);
+                if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D[r]->pa, data[r], s, 0, false);
+            }
         }
     }
     return rc;

@@ -20,6 +20,7 @@ struct VariantA {
     int vy, vz;      // radix-list variants of the y and z/2 axes
     size_t smem;     // dynamic shared memory per CTA
     const void *kfwd, *kinv;
+    const void *kfwd_x, *kinv_x;  // the same with the y columns in the exchange layout (or null)
 };
 
 struct VariantB {

@@ -737,7 +737,9 @@ __device__ __forceinline__ void cluster_wait() {
 // one has read the buffer (TileFFT::run's hook), so its loads overlap that
 // stage's arithmetic and stores.  Column tile 0 (the packed bins 0 and Nz/2)
 // keeps its own path.
-template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int CP = 0>
+// XCH: the y columns' global side (the forward's output, the inverse's
+// input) is the slab decomposition's exchange layout (PassAParams::xch).
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int CP = 0, bool XCH = false>
 __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned char *smem_raw, const int crank,
                                                 const int K, const int first_plane, const int plane_step) {
     using V = cx_t<T>;
@@ -769,35 +771,48 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
 
     // ---------------- y columns of plane g (whole CTA) ----------------
     // CP: copies of column tile t (t >= 1) of plane g into the tile buffer
-    auto prefetch_cols = [&](V *g, int t) {
+    // row n of plane g on the columns' global side: the exchange layout
+    // (XCH) or the field itself
+    auto xrow = [&](V *g, int plane, int n) -> V * {
+        if constexpr (XCH) {
+            const int s = n / P.xch_nyl;
+            return reinterpret_cast<V *>(P.xch) + s * P.xch_chunk +
+                   ((long long)plane * P.xch_nyl + (n - s * P.xch_nyl)) * NH;
+        } else {
+            return g + (long long)n * NH;
+        }
+    };
+    // where the columns read from and write to
+    auto in_row = [&](V *g, int plane, int n) -> V * { return FWD ? g + (long long)n * NH : xrow(g, plane, n); };
+    auto out_row = [&](V *g, int plane, int n) -> V * { return FWD ? xrow(g, plane, n) : g + (long long)n * NH; };
+    auto prefetch_cols = [&](V *g, int plane, int t) {
         const int c0 = t * WY;
         const int wv = min(WY, M - c0);
         for (int q = threadIdx.x; q < NY * WY; q += NT) {
             const int n = q / WY, w = q % WY;
-            cp_async_elem(tile + ColL::idx(n, w), g + (long long)n * NH + c0 + (w < wv ? w : 0), w < wv);
+            cp_async_elem(tile + ColL::idx(n, w), in_row(g, plane, n) + c0 + (w < wv ? w : 0), w < wv);
         }
         cp_async_commit();
     };
-    auto cols = [&](V *g) {
+    auto cols = [&](V *g, int plane) {
         if constexpr (CP) {
-            if (crank != 0 && crank < ntiles_y) prefetch_cols(g, crank);
+            if (crank != 0 && crank < ntiles_y) prefetch_cols(g, plane, crank);
         }
         for (int t = crank; t < ntiles_y; t += K) {
             const int c0 = t * WY;
             const int wv = min(WY, M - c0);
-            V *gc = g + c0;
             auto src = [&](int n, int w) -> V {
-                return (w < wv) ? ld_g(gc + (long long)n * NH + w) : V{(T)0, (T)0};
+                return (w < wv) ? ld_g(in_row(g, plane, n) + c0 + w) : V{(T)0, (T)0};
             };
             auto dst = [&](int n, int w, V v) {
-                if (w < wv) st_g(gc + (long long)n * NH + w, v);
+                if (w < wv) st_g(out_row(g, plane, n) + c0 + w, v);
             };
             if (CP && c0 != 0) {
                 cp_async_wait<0>();
                 // (the first stage begins with a block barrier)
                 const int tn = t + K;
                 auto refill = [&]() {
-                    if (tn < ntiles_y) prefetch_cols(g, tn);
+                    if (tn < ntiles_y) prefetch_cols(g, plane, tn);
                 };
                 FromSmem fs;
                 ColFFT::run(fs, dst, tile, sty, refill);
@@ -812,12 +827,13 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
                     const int n = q / WY, w = q % WY;
                     if (w >= wv) continue;
                     const V c1 = tile[ColL::idx(n, w)];
+                    V *orow = out_row(g, plane, n);
                     if (w == 0) {
                         const V c2 = c_conj(tile[ColL::idx((NY - n) % NY, 0)]);
-                        st_g(g + (long long)n * NH, c_scale(c_add(c1, c2), hf));
-                        st_g(g + (long long)n * NH + M, c_rot<true>(c_scale(c_sub(c1, c2), hf)));
+                        st_g(orow, c_scale(c_add(c1, c2), hf));
+                        st_g(orow + M, c_rot<true>(c_scale(c_sub(c1, c2), hf)));
                     } else {
-                        st_g(gc + (long long)n * NH + w, c1);
+                        st_g(orow + c0 + w, c1);
                     }
                 }
             } else {
@@ -827,12 +843,13 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
                 __syncthreads();
                 for (int n = threadIdx.x; n <= NY / 2; n += NT) {
                     const int n2 = (NY - n) % NY;
-                    const V a1 = ld_g(g + (long long)n * NH), a2 = ld_g(g + (long long)n2 * NH);
-                    const V b1 = ld_g(g + (long long)n * NH + M), b2 = ld_g(g + (long long)n2 * NH + M);
+                    V *r1 = in_row(g, plane, n), *r2 = in_row(g, plane, n2);
+                    const V a1 = ld_g(r1), a2 = ld_g(r2);
+                    const V b1 = ld_g(r1 + M), b2 = ld_g(r2 + M);
                     const V ha = c_scale(c_add(a1, c_conj(a2)), hf);
                     const V hb = c_scale(c_add(b1, c_conj(b2)), hf);
-                    st_g(g + (long long)n * NH, V{ha.x - hb.y, ha.y + hb.x});
-                    if (n2 != n) st_g(g + (long long)n2 * NH, V{ha.x + hb.y, -ha.y + hb.x});
+                    st_g(r1, V{ha.x - hb.y, ha.y + hb.x});
+                    if (n2 != n) st_g(r2, V{ha.x + hb.y, -ha.y + hb.x});
                 }
                 __syncthreads();
                 ColFFT::run(src, dst, tile, sty);
@@ -840,7 +857,7 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
             if constexpr (CP) {
                 if (c0 == 0 && t + K < ntiles_y) {
                     __syncthreads();  // tile 0's last reads of the buffer are done
-                    prefetch_cols(g, t + K);
+                    prefetch_cols(g, plane, t + K);
                 }
             }
         }
@@ -943,7 +960,7 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
         if (FWD) {
             if (do_rows) rows(g);
         } else if (do_cols) {
-            cols(g);
+            cols(g, plane);
         }
         __syncthreads();
         if (K > 1 && P.phases == 0) {
@@ -951,7 +968,7 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
             cluster_wait();
         }
         if (FWD) {
-            if (do_cols) cols(g);
+            if (do_cols) cols(g, plane);
         } else if (do_rows) {
             rows(g);
         }
@@ -959,12 +976,13 @@ __device__ __forceinline__ void pass_a_fast_run(const PassAParams &P, unsigned c
     }
 }
 
-template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB, int CP = 0>
+template <typename T, int NY, int M, int RW, int WY, int NT, bool FWD, int VY, int VZ, int MINB, int CP = 0,
+          bool XCH = false>
 __global__ void __launch_bounds__(NT, MINB) pass_a_fast(PassAParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = P.K;
-    pass_a_fast_run<T, NY, M, RW, WY, NT, FWD, VY, VZ, CP>(P, smem_raw, (int)blockIdx.x % K, K,
-                                                           (int)blockIdx.x / K, (int)gridDim.x / K);
+    pass_a_fast_run<T, NY, M, RW, WY, NT, FWD, VY, VZ, CP, XCH>(P, smem_raw, (int)blockIdx.x % K, K,
+                                                                (int)blockIdx.x / K, (int)gridDim.x / K);
 }
 
 // ---------------------------------------------------------------------------

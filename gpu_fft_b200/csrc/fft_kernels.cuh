@@ -73,6 +73,13 @@ struct PassAParams {
     // launched one after the other without clusters; K then only splits the
     // work of a plane between CTAs)
     int phases;
+    // slab decomposition, exchange layout (the XCH kernels): the forward's
+    // y-column results go to, and the inverse's y-column inputs come from,
+    // chunk y / xch_nyl of xch at element (plane * xch_nyl + y % xch_nyl) * Nh
+    // + kz -- the all-to-all's send/receive layout, so no pack or unpack copy
+    void *xch;
+    int xch_nyl;
+    long long xch_chunk;  // complex elements per chunk
 };
 
 struct PassBParams {

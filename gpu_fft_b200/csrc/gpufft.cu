@@ -268,7 +268,8 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
     for (int i = 0; i < nb && !P.fb; ++i)
         if (b_eligible(P, vb[i]) && seen++ == idx_b) P.fb = &vb[i];
     if (P.fa) {
-        for (const void *k : {P.fa->kfwd, P.fa->kinv}) {
+        for (const void *k : {P.fa->kfwd, P.fa->kinv, P.fa->kfwd_x, P.fa->kinv_x}) {
+            if (!k) continue;
             cudaError_t e = raise_smem_limit(k, P.fa->smem);
             if (e != cudaSuccess) {
                 cudaGetLastError();
@@ -290,8 +291,8 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         if (P.kfix > 0 && P.fa->kind == 0) {
             K = std::min(P.kfix, std::max(1, ny));
             if (K > 8) {
-                cudaFuncSetAttribute(P.fa->kfwd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-                cudaFuncSetAttribute(P.fa->kinv, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                for (const void *k : {P.fa->kfwd, P.fa->kinv, P.fa->kfwd_x, P.fa->kinv_x})
+                    if (k) cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             }
         }
         // split Pass A: z rows and y columns as two plain launches (the plane
@@ -712,18 +713,34 @@ int plan_destroy(Plan *P) {
     return GPUFFT_SUCCESS;
 }
 
+// xch (optional, specialised kernels only): the y columns' global side in
+// the slab decomposition's exchange layout (PassAParams::xch)
+struct XchLayout {
+    void *buf;
+    int nyl;
+    long long chunk;  // complex elements
+};
+
 template <typename T>
-static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
+static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, const XchLayout *xch = nullptr) {
     PassAParams prm = P.pa;
     prm.data = data;
+    const void *kf = P.fa ? P.fa->kfwd : nullptr, *ki = P.fa ? P.fa->kinv : nullptr;
+    if (xch) {
+        if (!P.fa || !P.fa->kfwd_x) return set_error(GPUFFT_ERR_UNSUPPORTED, "no exchange-layout Pass A kernel");
+        prm.xch = xch->buf;
+        prm.xch_nyl = xch->nyl;
+        prm.xch_chunk = xch->chunk;
+        kf = P.fa->kfwd_x;
+        ki = P.fa->kinv_x;
+    }
     if (P.fa && P.split_a) {
         // forward: z rows then y columns; inverse: y columns then z rows
         prm.K = P.k_fa;
         void *args[] = {&prm};
         for (int half = 0; half < 2; ++half) {
             prm.phases = (fwd == (half == 0)) ? 1 : 2;
-            const cudaError_t e = cudaLaunchKernel(fwd ? P.fa->kfwd : P.fa->kinv, dim3(P.grid_fa), dim3(P.fa->nt), args,
-                                                   P.fa->smem, s);
+            const cudaError_t e = cudaLaunchKernel(fwd ? kf : ki, dim3(P.grid_fa), dim3(P.fa->nt), args, P.fa->smem, s);
             if (e != cudaSuccess) return cuda_error(e, "launch split pass A (specialised)");
         }
         return GPUFFT_SUCCESS;
@@ -744,7 +761,7 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         void *args[] = {&prm};
-        const cudaError_t e = cudaLaunchKernelExC(&cfg, fwd ? P.fa->kfwd : P.fa->kinv, args);
+        const cudaError_t e = cudaLaunchKernelExC(&cfg, fwd ? kf : ki, args);
         return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass A (specialised)");
     }
     cudaLaunchConfig_t cfg = {};
@@ -836,6 +853,19 @@ static int plan_exec_pass_impl(const Plan *P, void *data, void *stream, int pass
     if (P->dtype == GPUFFT_FLOAT)
         return pass == 0 ? launch_pass_a<float>(*P, data, s, forward) : launch_pass_b<float>(*P, data, s, forward);
     return pass == 0 ? launch_pass_a<double>(*P, data, s, forward) : launch_pass_b<double>(*P, data, s, forward);
+}
+
+bool plan_has_xch(const Plan *P) { return P && P->fa && P->fa->kfwd_x && P->fa->kinv_x; }
+
+int plan_exec_pass_a_xch(const Plan *P, void *data, void *xch, int nyl, long long chunk, void *stream, bool forward) {
+    if (!P) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    if (!data || !xch) return set_error(GPUFFT_ERR_INVALID, "data or exchange buffer is NULL");
+    if (nyl < 1 || P->ny % nyl != 0) return set_error(GPUFFT_ERR_INVALID, "Ny = %lld is not a multiple of %d",
+                                                      (long long)P->ny, nyl);
+    const XchLayout x{xch, nyl, chunk};
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->dtype == GPUFFT_FLOAT ? launch_pass_a<float>(*P, data, s, forward, &x)
+                                    : launch_pass_a<double>(*P, data, s, forward, &x);
 }
 
 int plan_launches(const Plan *P) { return P ? (P->nx == 1 ? 1 : 2) + (P->fa && P->split_a ? 1 : 0) : 0; }

@@ -50,6 +50,12 @@ int plan_exec(const Plan *P, void *data, void *stream, bool forward);
 int plan_exec_ex(const Plan *P, void *data, void *stream, bool forward, double scale, int dealias);
 int plan_exec_pass(const Plan *P, void *data, void *stream, int pass, bool forward);
 int plan_launches(const Plan *P);
+// Slab decomposition: whether P's Pass A has exchange-layout kernels, and a
+// Pass A whose y columns write (forward) or read (inverse) the all-to-all's
+// layout in `xch` -- chunk y / nyl, element (x * nyl + y % nyl) * Nh + kz --
+// instead of the field
+bool plan_has_xch(const Plan *P);
+int plan_exec_pass_a_xch(const Plan *P, void *data, void *xch, int nyl, long long chunk, void *stream, bool forward);
 int plan_describe(const Plan *P, char *buf, int len);
 int plan_autotune(Plan *P, void *scratch, void *stream);
 // P takes Q's kernel choice (same grid, precision and form; Q tuned already)
