@@ -7,15 +7,18 @@
 // a 2D cuFFT per plane, a transpose into a field-sized buffer, MPI
 // point-to-point exchanges, a chunk transpose and a strided 1D cuFFT.  Here a
 // rank runs
-//   R2C:  Pass A on its Nx/p planes (in place)
-//         -> pack the Ny/p rows of each plane bound for rank s into chunk s of
-//            a send buffer (one 2D copy per destination)
+//   R2C:  Pass A on its Nx/p planes, its y columns stored straight into a
+//            send buffer: the Ny/p rows of each plane bound for rank s in
+//            chunk s (the specialised kernels' exchange-layout form; with the
+//            generic kernels Pass A runs in place and a 2D copy per
+//            destination packs the chunks)
 //         -> one all-to-all: chunk s goes to rank s, landing in the user's
 //            buffer as block r of the y-slab [X][yl][kz] (the layout Pass B
 //            reads; no chunk transpose)
 //         -> Pass B over the Nx-point columns of the y-slab (stride (Ny/p)*Nh);
 //   C2R:  the mirror image (Pass B inverse, all-to-all into the send buffer,
-//         unpack into the x-slab, Pass A inverse).
+//         Pass A inverse reading its y columns from there, or unpack copies
+//         and Pass A in place).
 // Pass A is the single-GPU plan of an (Nx/p, Ny, Nz) grid and Pass B the one
 // of an (Nx, Ny/p, Nz) grid, so the kernels, their autotuning and their
 // parity tests are the single-GPU ones.
