@@ -60,6 +60,10 @@ static int hostpipe_create(HostPipe **out, Plan *plan, int depth) {
     *out = nullptr;
     if (!plan) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
     if (depth < 1 || depth > 8) return set_error(GPUFFT_ERR_INVALID, "depth %d is outside 1..8", depth);
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != plan->device)
+        return set_error(GPUFFT_ERR_INVALID, "the plan belongs to device %d: make it current before creating the pipe",
+                         plan->device);
     HostPipe *H = new (std::nothrow) HostPipe();
     if (!H) return set_error(GPUFFT_ERR_OOM, "host allocation failed");
     H->plan = plan;
