@@ -39,6 +39,7 @@ EXPORTS = (
     "gpufft_exec16_c2r", "gpufft_exec16_pass", "gpufft_quantize16", "gpufft_dequantize16",
     "gpufft_server_create", "gpufft_server_stop", "gpufft_server_destroy", "gpufft_server_prepare",
     "gpufft_server_submit", "gpufft_server_poll", "gpufft_server_wait", "gpufft_server_cancel", "gpufft_server_stats",
+    "gpufft_server_release",
     "gpufft_init_dist", "gpufft_dist_unique_id", "gpufft_dplan_create", "gpufft_dplan_destroy", "gpufft_dexec_r2c", "gpufft_dexec_c2r",
     "gpufft_dplan_layout", "gpufft_dgroup_create", "gpufft_dgroup_exec",
 )
@@ -60,7 +61,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("cancelled", ctypes.c_int64),
                 ("queued", ctypes.c_int64), ("in_flight", ctypes.c_int64), ("max_in_flight", ctypes.c_int64),
                 ("bytes_in_use", ctypes.c_int64), ("peak_bytes_in_use", ctypes.c_int64), ("plans", ctypes.c_int64),
-                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double)]
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("records", ctypes.c_int64)]
 
 
 class GpuFFTError(RuntimeError):
@@ -130,6 +131,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_server_poll.argtypes = [vp, i64, ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_double)]
     lib.gpufft_server_wait.argtypes = [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     lib.gpufft_server_cancel.argtypes = [vp, i64]
+    lib.gpufft_server_release.argtypes = [vp, i64]
     lib.gpufft_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
     lib.gpufft_dist_unique_id.argtypes = [vp]
     lib.gpufft_init_dist.argtypes = [i64, i64, i64, ci, ci, ci, vp]
@@ -619,6 +621,10 @@ class Server:
 
     def cancel(self, rid: int) -> None:
         _check(load_library().gpufft_server_cancel(self._h, rid))
+
+    def release(self, rid: int) -> None:
+        """Drops the record of a finished request (for clients that poll instead of waiting)."""
+        _check(load_library().gpufft_server_release(self._h, rid))
 
     def stats(self) -> dict:
         st = ServerStats()

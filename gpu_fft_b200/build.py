@@ -15,8 +15,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpufft_b200.so")
 
-SOURCES = ["gpufft.cu", "fast_f32.cu", "fast_f64.cu", "noalloc.cu", "batch.cu", "s16.cu", "serve.cu", "dist.cu", "fast_f32_3s.cu", "hostpipe.cu"]
-HEADERS = ["fft_kernels.cuh", "fft_radix.cuh", "fft_fast.cuh", "fft_s16.cuh", "fast_registry.h", "fast_entries.h", "gpufft_internal.h"]
+SOURCES = ["gpufft.cu", "fast_f32.cu", "fast_f64.cu", "noalloc.cu", "batch.cu", "s16.cu", "serve.cu", "dist.cu", "fast_f32_3s.cu", "hostpipe.cu", "fast_queue.cu"]
+HEADERS = ["fft_kernels.cuh", "fft_radix.cuh", "fft_fast.cuh", "fft_s16.cuh", "fft_queue.cuh", "fast_registry.h", "fast_entries.h", "gpufft_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 

@@ -13,6 +13,8 @@ namespace fast {
 struct VariantA {
     int kind;        // 0: plane exchanged through L2 (cluster size chosen at plan time)
                      // 1: plane held in the cluster's shared memory (cluster size = k)
+                     // 2: persistent queue of row and column items fed by bulk / tensor
+                     //    copies (fft_queue.cuh; k = ring depth, nt counts the copy-issuing warp)
     int k;           // cluster size of kind 1
     int dtype;       // GPUFFT_FLOAT / GPUFFT_DOUBLE
     int ny, m;       // Ny and Nz/2
@@ -43,6 +45,8 @@ extern const VariantA kVariantsA_f32s[];  // 3-smooth lengths (fast_f32_3s.cu)
 extern const int kNumVariantsA_f32s;
 extern const VariantB kVariantsB_f32s[];
 extern const int kNumVariantsB_f32s;
+extern const VariantA kVariantsA_f32q[];  // queue-scheduled Pass A (fast_queue.cu)
+extern const int kNumVariantsA_f32q;
 extern const VariantA kVariantsA_f64[];
 extern const int kNumVariantsA_f64;
 extern const VariantB kVariantsB_f64[];

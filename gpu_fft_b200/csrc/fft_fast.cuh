@@ -92,8 +92,10 @@ __host__ __device__ constexpr int stage_offset(const Fac &f, int s) {
     return off;
 }
 
-// which threads cooperate on a tile: the whole CTA, or one warp
-enum Scope { BLOCK = 0, WARP = 1 };
+// which threads cooperate on a tile: the whole CTA, one warp, or the first
+// NT threads of the CTA (GROUP: named barrier 1, so a CTA can run other warps
+// -- a copy-issuing warp -- beside the ones that transform the tile)
+enum Scope { BLOCK = 0, WARP = 1, GROUP = 2 };
 
 // shared-memory layouts of a tile of W sequences of length N
 //  COLS: element (n, w) at n*W + w             (columns contiguous in w)
@@ -184,11 +186,14 @@ struct TileFFT {
     static constexpr Fac F = factor(N, VARIANT);
     static constexpr int NS = F.n;
     static_assert(NS >= 0, "length must factor into 2,3,5,7,11,13");
-    static_assert(SCOPE == BLOCK || NT == 32, "a warp-scope tile has 32 threads");
+    static_assert(SCOPE != WARP || NT == 32, "a warp-scope tile has 32 threads");
+    static_assert(SCOPE != GROUP || NT % 32 == 0, "a group-scope tile has whole warps");
 
     static __device__ __forceinline__ void sync() {
         if constexpr (SCOPE == WARP)
             __syncwarp();
+        else if constexpr (SCOPE == GROUP)
+            asm volatile("bar.sync 1, %0;\n" ::"n"(NT) : "memory");
         else
             __syncthreads();
     }

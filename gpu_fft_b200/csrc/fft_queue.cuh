@@ -1,0 +1,459 @@
+// fft_queue.cuh — Pass A (z R2C/C2R + y C2C of every x-plane) as one
+// persistent, queue-scheduled kernel whose inputs arrive by bulk and tensor
+// copies (sm_100a: cp.async.bulk / cp.async.bulk.tensor completing on
+// mbarriers).
+//
+// Replaces the reference's batched 2D cuFFT R2C/C2R over x-planes
+// (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT_init.cu:61-64,90-91, executed at
+// GPU_FFT/src/FFT_implementation/FFT_R2C.cu:45 and FFT_C2R.cu:66).
+//
+// Work items.  A plane (Ny rows of Nh = M+1 complex, M = Nz/2) is cut into
+//   * row items: RI consecutive z-rows (one contiguous span of the field,
+//     fetched by ONE 1D bulk copy), each row's M-point FFT plus the
+//     real-to-complex unpack (forward) or pack (inverse) done by half a warp
+//     in shared memory;
+//   * column items: WY consecutive kz columns of all Ny rows, the y FFT,
+//     fetched by TWO 2D tensor copies over a "row pair" view of the field:
+//     with Nh odd, two rows are 16*Nh bytes, so rows 2r and 2r+1 form one
+//     16-byte-aligned line of 2*Nh complex.  Box E (WY wide at x = c0) holds
+//     the even rows' columns; box O (WY+2 wide at x = Nh-1+c0, the odd row's
+//     first column rounded down to 16 bytes) holds the odd rows' columns one
+//     slot in.  Slots read beyond the tile are ignored (another item may be
+//     writing them).  The inverse's tile 0 also needs bin M of every row:
+//     even rows find it in box O's slot 0, odd rows in a third 2-wide box.
+// The forward runs row items then column items of a plane (the intermediate
+// plane stays in place, in L2), the inverse the reverse.
+//
+// Schedule.  The item list (built on the host) interleaves the first-phase
+// items of plane b with the second-phase items of plane b - D, so that only
+// about D planes are between their phases at any time (the intermediate
+// stays in L2; one cluster per plane put 40-70 planes there).  CTAs claim
+// items in list order from an atomic counter.  A second-phase item waits
+// (acquire load of the plane's completion count, bounded by a time limit,
+// then an error flag) until its plane's first phase is complete; first-
+// phase items publish with a release add after their stores.
+//
+// CTA roles: NT/32 consumer warps transform items; one producer warp (lane
+// 0) claims the next item, waits for its plane when needed and issues its
+// copies into the next free buffer of an NBUF-deep ring (full/empty
+// mbarrier pairs), so an item's loads are in flight while the consumers
+// transform the previous one and no load occupies a register.
+//
+// Deadlock freedom: a CTA waits for a plane only in its producer, while its
+// consumers finish every item the CTA claimed earlier (they never wait on
+// anything but copies already issued).  Items are claimed in list order, so
+// the lowest-numbered unfinished item always belongs to a CTA that can
+// finish it: its dependencies have lower numbers and are finished.  This
+// holds however many CTAs are resident.
+//
+// Counters (plan-owned, int): [0] next item, [1] CTAs finished, [2] error
+// flag, [3] spare, [4 + x] items finished of plane x.  The last CTA to finish
+// zeroes [0], [1] and the plane counts for the next launch, so one plan's
+// executions must not overlap on the GPU.
+#pragma once
+#include <cuda.h>
+
+#include "fft_fast.cuh"
+
+namespace gpufft {
+namespace q {
+
+using fast::TileFFT;
+using fast::COLS;
+using fast::GROUP;
+using fast::FromSmem;
+using fast::ToSmem;
+
+struct PassAQParams {
+    void *data;
+    const void *unp;    // exp(-2 pi i k / Nz), k < M (the full unpack table)
+    const void *stz;    // per-stage tables of the z and y FFTs (fft_fast.cuh stage_offset)
+    const void *sty;
+    const int *items;   // work list: (plane << 16) | (type << 15) | sub
+    int nitems;
+    int *ctr;           // counters (header)
+    int need;           // first-phase items per plane
+    long long wait_ns;  // time limit of one dependency or copy wait
+};
+
+enum ItemType { ROW_ITEM = 0, COL_ITEM = 1 };
+__host__ __device__ constexpr int item_code(int plane, int type, int sub) { return (plane << 16) | (type << 15) | sub; }
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes the initialised barriers visible to the copy engine
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Waits for the phase of parity `parity` to complete; false once `limit_ns`
+// has passed without it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (true) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if ((long long)(globaltimer() - t0) > limit_ns) return false;
+    }
+}
+// generic-proxy accesses before this point are ordered before later copies
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+// 1D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// 2D tensor copy global -> shared of the box at (x, y) of `map` (no multicast)
+__device__ __forceinline__ void tensor_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(int *p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void group_sync() {
+    asm volatile("bar.sync 1, %0;\n" ::"n"(N) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// shape of one instantiation
+// ---------------------------------------------------------------------------
+template <typename T, int NY, int M, int NT, int NBUF>
+struct QShape {
+    using V = cx_t<T>;
+    static constexpr int NH = M + 1;
+    static constexpr int WY = 128 / (int)sizeof(V);  // columns per column item (128-byte rows)
+    static constexpr int RI = 32;                    // rows per row item
+    static constexpr int BH = NY / 2;                // row pairs per box
+    static constexpr int NRI = NY / RI;
+    static constexpr int NCI = M / WY;
+    static constexpr int E_BYTES = WY * BH * (int)sizeof(V);
+    static constexpr int O_BYTES = (WY + 2) * BH * (int)sizeof(V);
+    static constexpr int X_BYTES = 2 * BH * (int)sizeof(V);
+    static constexpr int ROW_BYTES = RI * NH * (int)sizeof(V);
+    static constexpr int TILE_BYTES = NY * WY * (int)sizeof(V);
+    static constexpr int rup(int v) { return (v + 127) / 128 * 128; }
+    static constexpr int mx(int a, int b) { return a > b ? a : b; }
+    static constexpr int O_OFF = rup(E_BYTES);
+    static constexpr int X_OFF = O_OFF + rup(O_BYTES);
+    static constexpr int BUF = rup(mx(mx(ROW_BYTES, TILE_BYTES), X_OFF + X_BYTES));
+    static constexpr int TAB = rup((M + M + NY) * (int)sizeof(V));
+    // tables, buffers, mbarriers, slot words, and slack for 128-byte alignment
+    static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + 2 * NBUF * 8 + NBUF * 4 + 128; }
+    static_assert(sizeof(V) == 8, "row-pair view: FP32 complex");
+    static_assert(NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
+    static_assert(NY % RI == 0 && NY % 2 == 0 && BH <= 256, "rows per item / box height");
+    static_assert(M % WY == 0, "whole column tiles");
+    static_assert(M == 256, "the row FFT is 16 x 16");
+    static_assert(NT == 32 * (RI / 2), "two rows per consumer warp");
+};
+
+// ---------------------------------------------------------------------------
+// one warp, two z-rows of M = 256 complex (16 lanes per row), in place in
+// the natural row layout.  Step 1: lane a transforms x[a + 16 n] over n and
+// twiddles by w_256^(a f); its outputs go to slot 16 f + (a ^ f) (an XOR
+// swizzle: the writes of step 1 and the reads of step 2 are both
+// conflict-free).  Step 2: lane b transforms those of frequency b over a,
+// giving X[b + 16 j] in registers.  The per-stage table (stage 1 of the
+// 16 x 16 factorisation) holds w_256^(j k) at 15 + (j - 1) 16 + k, and the
+// twiddle is symmetric in (j, k): lane a reads entry (f, a), contiguous
+// across lanes.
+// ---------------------------------------------------------------------------
+template <bool FWD, typename V>
+__device__ __forceinline__ void row256_step1(V (&x)[16], V *row, const V *stz, int a) {
+    Dft<16, FWD, V>::run(x);
+#pragma unroll
+    for (int f = 1; f < 16; ++f) x[f] = c_tw<FWD>(x[f], stz[15 + (f - 1) * 16 + a]);
+    __syncwarp();  // every lane has read its inputs before the row is overwritten
+#pragma unroll
+    for (int f = 0; f < 16; ++f) row[16 * f + (a ^ f)] = x[f];
+    __syncwarp();
+}
+template <bool FWD, typename V>
+__device__ __forceinline__ void row256_step2(V (&x)[16], const V *row, int b) {
+#pragma unroll
+    for (int a = 0; a < 16; ++a) x[a] = row[16 * b + (a ^ b)];
+    Dft<16, FWD, V>::run(x);
+}
+
+// ---------------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------------
+template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF>
+__global__ void __launch_bounds__(NT + 32, 1)
+    pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
+                 const __grid_constant__ CUtensorMap tm_x) {
+    using S = QShape<T, NY, M, NT, NBUF>;
+    using V = cx_t<T>;
+    using ColFFT = TileFFT<T, NY, S::WY, NT, FWD, COLS, VY, GROUP>;
+    using ColL = typename ColFFT::L;
+    constexpr int NH = S::NH, WY = S::WY, RI = S::RI, BH = S::BH;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // copy destinations are 128-byte aligned (smem_bytes() reserves the slack)
+    unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    V *unp = reinterpret_cast<V *>(smem);
+    V *stz = unp + M;
+    V *sty = stz + M;
+    unsigned char *bufs = smem + S::TAB;
+    uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF);
+    uint64_t *empty = full + NBUF;
+    int *info = reinterpret_cast<int *>(empty + NBUF);
+
+    for (int q = threadIdx.x; q < M; q += blockDim.x) unp[q] = reinterpret_cast<const V *>(P.unp)[q];
+    for (int q = threadIdx.x; q < M - 1; q += blockDim.x) stz[q] = reinterpret_cast<const V *>(P.stz)[q];
+    for (int q = threadIdx.x; q < NY - 1; q += blockDim.x) sty[q] = reinterpret_cast<const V *>(P.sty)[q];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NBUF; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    V *field = reinterpret_cast<V *>(P.data);
+    int *ctr = P.ctr;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int first_type = FWD ? ROW_ITEM : COL_ITEM;  // the phase that publishes
+
+    if (warp == NT / 32) {
+        // ------------------------------ producer ------------------------------
+        if (lane == 0) {
+            bool err = false;
+            for (int k = 0;; ++k) {
+                const int s = k % NBUF;
+                const uint32_t ph = (uint32_t)((k / NBUF) & 1);
+                if (!mbar_wait(&empty[s], ph ^ 1u, P.wait_ns)) {
+                    err = true;
+                    info[s] = -1;
+                    mbar_arrive(&full[s]);  // consumers may be waiting for this slot
+                    break;
+                }
+                const int g = atomicAdd(&ctr[0], 1);
+                const int it = g < P.nitems ? P.items[g] : -1;
+                info[s] = it;
+                if (it < 0) {
+                    mbar_arrive(&full[s]);
+                    break;
+                }
+                const int plane = it >> 16, type = (it >> 15) & 1, sub = it & 0x7fff;
+                if (type != first_type) {
+                    const int *cnt = &ctr[4 + plane];
+                    if (ld_acquire(cnt) < P.need) {
+                        const unsigned long long t0 = globaltimer();
+                        while (ld_acquire(cnt) < P.need) {
+                            __nanosleep(200);
+                            // once any CTA has given up, the others stop waiting too
+                            if ((long long)(globaltimer() - t0) > P.wait_ns || ld_acquire(&ctr[2]) != 0) {
+                                err = true;  // go on: wrong results, no hang
+                                break;
+                            }
+                        }
+                    }
+                    fence_proxy_async_global();
+                }
+                fence_proxy_async_shared();  // the consumers' accesses to buffer s come first
+                unsigned char *b = bufs + (size_t)s * S::BUF;
+                if (type == ROW_ITEM) {
+                    mbar_arrive_expect_tx(&full[s], (uint32_t)S::ROW_BYTES);
+                    bulk_load(b, field + ((long long)plane * NY + (long long)sub * RI) * NH, (uint32_t)S::ROW_BYTES,
+                              &full[s]);
+                } else {
+                    const int c0 = sub * WY;
+                    const int y = plane * BH;
+                    const bool xtra = !FWD && sub == 0;
+                    mbar_arrive_expect_tx(&full[s], (uint32_t)(S::E_BYTES + S::O_BYTES + (xtra ? S::X_BYTES : 0)));
+                    tensor_load_2d(b, &tm_e, c0, y, &full[s]);
+                    tensor_load_2d(b + S::O_OFF, &tm_o, NH - 1 + c0, y, &full[s]);
+                    if (xtra) tensor_load_2d(b + S::X_OFF, &tm_x, 2 * NH - 2, y, &full[s]);
+                }
+            }
+            if (err) atomicExch(&ctr[2], 1);
+        }
+    } else {
+        // ------------------------------ consumers ------------------------------
+        const int tid = threadIdx.x;
+        for (int k = 0;; ++k) {
+            const int s = k % NBUF;
+            const uint32_t ph = (uint32_t)((k / NBUF) & 1);
+            if (!mbar_wait(&full[s], ph, P.wait_ns)) {
+                // a copy that never completed: flag it, give it one more time
+                // limit so that no copy is left in flight at exit, and stop
+                if (tid == 0) atomicExch(&ctr[2], 1);
+                mbar_wait(&full[s], ph, P.wait_ns);
+                break;
+            }
+            const int it = info[s];
+            if (it < 0) break;
+            const int plane = it >> 16, type = (it >> 15) & 1, sub = it & 0x7fff;
+            unsigned char *b = bufs + (size_t)s * S::BUF;
+            V *gplane = field + (long long)plane * NY * NH;
+            if (type == ROW_ITEM) {
+                // two rows per warp: lanes 0-15 row 2w, lanes 16-31 row 2w+1
+                const int h = lane >> 4, a = lane & 15;
+                const int r = 2 * warp + h;
+                V *row = reinterpret_cast<V *>(b) + r * NH;
+                V *grow = gplane + ((long long)sub * RI + r) * NH;
+                V x[16];
+                if constexpr (FWD) {
+#pragma unroll
+                    for (int n = 0; n < 16; ++n) x[n] = row[a + 16 * n];
+                    row256_step1<true>(x, row, stz, a);
+                    row256_step2<true>(x, row, a);
+                    __syncwarp();  // step 2's reads are done before X is stored
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) row[a + 16 * j] = x[j];
+                    __syncwarp();
+                    // unpack: X[k] = E + O, E = (Z[k] + conj Z[M-k]) / 2,
+                    // O = -i w^k (Z[k] - conj Z[M-k]) / 2; bins 0 and M packed in slot 0
+                    const T hf = (T)0.5;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int kk = a + 16 * j;
+                        const V za = x[j];
+                        const V zb = c_conj(row[(M - kk) & (M - 1)]);
+                        const V e = c_scale(c_add(za, zb), hf);
+                        const V d = c_scale(c_sub(za, zb), hf);
+                        const V o = c_rot<true>(c_mul(d, unp[kk]));
+                        const V xa = c_add(e, o);
+                        if (kk == 0) {
+                            const V xb = c_conj(c_sub(e, o));
+                            st_g(grow, V{xa.x, xb.x});
+                        } else {
+                            st_g(grow + kk, xa);
+                        }
+                    }
+                } else {
+                    // pack: Z[k] = S + Pk, S = X[k] + conj X[M-k], Pk = i conj(w^k) (X[k] - conj X[M-k]);
+                    // slot 0 holds (Re X0, Re XM)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int kk = a + 16 * j;
+                        V xa = row[kk], xb = row[(M - kk) & (M - 1)];
+                        if (kk == 0) {
+                            xb = V{xa.y, (T)0};
+                            xa = V{xa.x, (T)0};
+                        }
+                        const V cm = c_conj(xb);
+                        const V sv = c_add(xa, cm);
+                        const V pk = c_rot<false>(c_mulc(c_sub(xa, cm), unp[kk]));
+                        x[j] = c_add(sv, pk);
+                    }
+                    row256_step1<false>(x, row, stz, a);
+                    row256_step2<false>(x, row, a);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) st_g(grow + a + 16 * j, x[j]);
+                    if (a == 0) st_g(grow + M, V{(T)0, (T)0});  // padding cells of the real row
+                }
+            } else {
+                // column item: y FFT of columns c0 .. c0 + WY - 1 of all NY rows
+                const int c0 = sub * WY;
+                const V *be = reinterpret_cast<const V *>(b);
+                const V *bo = reinterpret_cast<const V *>(b + S::O_OFF);
+                const V *bx = reinterpret_cast<const V *>(b + S::X_OFF);
+                V *tile = reinterpret_cast<V *>(b);
+                auto at = [&](int n, int w) -> V {
+                    return (n & 1) ? bo[(n >> 1) * (WY + 2) + 1 + w] : be[(n >> 1) * WY + w];
+                };
+                auto dst = [&](int n, int w, V v) { st_g(gplane + (long long)n * NH + c0 + w, v); };
+                if constexpr (FWD) {
+                    auto src = [&](int n, int w) -> V { return at(n, w); };
+                    if (sub != 0) {
+                        ColFFT::run(src, dst, tile, sty);
+                    } else {
+                        // column 0 carries (bin 0) + i (bin M); split after the FFT
+                        ToSmem ts;
+                        ColFFT::run(src, ts, tile, sty);
+                        group_sync<NT>();
+                        const T hf = (T)0.5;
+                        for (int qq = tid; qq < NY * WY; qq += NT) {
+                            const int n = qq / WY, w = qq % WY;
+                            const V c1 = tile[ColL::idx(n, w)];
+                            V *orow = gplane + (long long)n * NH;
+                            if (w == 0) {
+                                const V c2 = c_conj(tile[ColL::idx((NY - n) % NY, 0)]);
+                                st_g(orow, c_scale(c_add(c1, c2), hf));
+                                st_g(orow + M, c_rot<true>(c_scale(c_sub(c1, c2), hf)));
+                            } else {
+                                st_g(orow + w, c1);
+                            }
+                        }
+                    }
+                } else {
+                    // inverse, tile 0: the Hermitian projection of bins 0 (a) and M (b)
+                    // along y, packed as a' + i b' into column 0
+                    const T hf = (T)0.5;
+                    auto binm = [&](int n) -> V {
+                        return (n & 1) ? bx[(n >> 1) * 2 + 1] : bo[(n >> 1) * (WY + 2)];
+                    };
+                    auto src = [&](int n, int w) -> V {
+                        if (sub == 0 && w == 0) {
+                            const int n2 = (NY - n) % NY;
+                            const V ha = c_scale(c_add(at(n, 0), c_conj(at(n2, 0))), hf);
+                            const V hb = c_scale(c_add(binm(n), c_conj(binm(n2))), hf);
+                            return V{ha.x - hb.y, ha.y + hb.x};
+                        }
+                        return at(n, w);
+                    };
+                    ColFFT::run(src, dst, tile, sty);
+                }
+            }
+            group_sync<NT>();  // stores issued, buffer reads done
+            if (tid == 0) {
+                if (type == first_type) red_release_add(&ctr[4 + plane], 1);
+                mbar_arrive(&empty[s]);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctr[1], 1) == (int)gridDim.x - 1) {
+            // last CTA out: every other CTA is done with the counters
+            const int nx = P.nitems / (S::NRI + S::NCI);
+            for (int p = 0; p < nx; ++p) ctr[4 + p] = 0;
+            atomicExch(&ctr[0], 0);
+            atomicExch(&ctr[1], 0);
+            __threadfence();
+        }
+    }
+}
+
+}  // namespace q
+}  // namespace gpufft

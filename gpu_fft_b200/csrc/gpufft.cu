@@ -6,6 +6,8 @@
 // cuFFT plans and a field-sized scratch buffer it holds a radix factorisation
 // per axis, the tile shapes of the two passes, the cluster size of Pass A and
 // three FP64-computed twiddle tables (rounded once to the storage type).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +27,7 @@
 #include "../../include/gpufft_b200.h"
 #include "fft_fast.cuh"
 #include "fft_kernels.cuh"
+#include "fft_queue.cuh"
 #include "gpufft_internal.h"
 
 namespace gpufft {
@@ -222,6 +225,7 @@ static const std::vector<fast::VariantA> &variants_a(int dtype) {
     static const std::vector<fast::VariantA> f32 = [] {
         std::vector<fast::VariantA> v(fast::kVariantsA_f32, fast::kVariantsA_f32 + fast::kNumVariantsA_f32);
         v.insert(v.end(), fast::kVariantsA_f32s, fast::kVariantsA_f32s + fast::kNumVariantsA_f32s);
+        v.insert(v.end(), fast::kVariantsA_f32q, fast::kVariantsA_f32q + fast::kNumVariantsA_f32q);
         return v;
     }();
     static const std::vector<fast::VariantA> f64(fast::kVariantsA_f64, fast::kVariantsA_f64 + fast::kNumVariantsA_f64);
@@ -245,6 +249,112 @@ static bool b_eligible(const Plan &P, const fast::VariantB &v) {
     const int m = (int)(P.nz / 2);
     const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
     return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v == 2) == P.tc_split);
+}
+
+// ---------------------------------------------------------------------------
+// queue-scheduled Pass A (kind 2): item lists, counters, unpack table
+// ---------------------------------------------------------------------------
+static void free_queue(Plan &P) {
+    if (P.q_dev) cudaFree(P.q_dev);
+    P.q_dev = nullptr;
+    P.q_items_f = P.q_items_i = nullptr;
+    P.q_unp = nullptr;
+}
+
+// Work list of one direction: block b holds the first-phase items of plane b
+// (b < nx) interleaved with the second-phase items of plane b - depth
+// (b >= depth), so a plane's second phase is claimed about `depth` planes of
+// work after its first.
+static std::vector<int> queue_items(int nx, int nfirst, int nsecond, int first_type, int depth) {
+    std::vector<int> v;
+    v.reserve((size_t)nx * (nfirst + nsecond));
+    for (int b = 0; b < nx + depth; ++b) {
+        const int a = b < nx ? nfirst : 0;
+        const int c = b >= depth ? nsecond : 0;
+        const int tot = a + c;
+        int ia = 0, ic = 0;
+        for (int i = 0; i < tot; ++i) {
+            // spread the two kinds evenly through the block
+            const bool take_a = ic >= c || (ia < a && (long long)ia * tot <= (long long)i * a);
+            if (take_a)
+                v.push_back(q::item_code(b, first_type, ia++));
+            else
+                v.push_back(q::item_code(b - depth, 1 - first_type, ic++));
+        }
+    }
+    return v;
+}
+
+static int setup_queue(Plan &P) {
+    free_queue(P);
+    const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
+    const int ri = 32, wy = P.fa->wy;
+    const int nri = ny / ri, nci = m / wy;
+    int depth = P.kfix > 0 ? P.kfix : 8;
+    if (const char *ev = std::getenv("GPUFFT_QUEUE_DEPTH")) depth = std::atoi(ev);
+    depth = std::max(1, std::min(nx, depth));
+    const std::vector<int> fwd = queue_items(nx, nri, nci, q::ROW_ITEM, depth);
+    const std::vector<int> inv = queue_items(nx, nci, nri, q::COL_ITEM, depth);
+    std::vector<float> unp(2 * (size_t)m);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int k = 0; k < m; ++k) {
+        const long double ang = two_pi * (long double)k / (long double)(2 * m);
+        unp[2 * k] = (float)cosl(ang);
+        unp[2 * k + 1] = (float)(-sinl(ang));
+    }
+    const size_t cbytes = ((size_t)(4 + nx) * sizeof(int) + 255) / 256 * 256;
+    const size_t lbytes = (fwd.size() * sizeof(int) + 255) / 256 * 256;
+    const size_t ubytes = unp.size() * sizeof(float);
+    cudaError_t e = cudaMalloc(&P.q_dev, cbytes + 2 * lbytes + ubytes);
+    if (e != cudaSuccess) {
+        P.q_dev = nullptr;
+        return set_error(GPUFFT_ERR_OOM, "cudaMalloc Pass A queue state: %s", cudaGetErrorString(e));
+    }
+    char *b = (char *)P.q_dev;
+    e = cudaMemset(b, 0, cbytes);
+    if (e == cudaSuccess) e = cudaMemcpy(b + cbytes, fwd.data(), fwd.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b + cbytes + lbytes, inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b + cbytes + 2 * lbytes, unp.data(), ubytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        free_queue(P);
+        return cuda_error(e, "upload Pass A queue state");
+    }
+    P.q_depth = depth;
+    P.q_nitems = (int)fwd.size();
+    P.q_need = nri;
+    P.q_items_f = reinterpret_cast<const int *>(b + cbytes);
+    P.q_items_i = reinterpret_cast<const int *>(b + cbytes + lbytes);
+    P.q_unp = b + cbytes + 2 * lbytes;
+    return GPUFFT_SUCCESS;
+}
+
+// cuTensorMapEncodeTiled from the driver, found at run time (no libcuda link)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The row-pair view of an FP32 field with Nh odd: lines of 2*Nh 8-byte
+// elements (rows 2r and 2r+1), Nx*Ny/2 lines, line pitch 16*Nh bytes.
+static bool encode_pair_map(CUtensorMap *m, void *data, long long nh, long long lines, int box_w, int box_h) {
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)(2 * nh), (cuuint64_t)lines};
+    const cuuint64_t strides[1] = {(cuuint64_t)(2 * nh * 8)};
+    const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+    const cuuint32_t es[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, data, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Picks the specialised kernels for this plan's shape (first registry entry,
@@ -278,7 +388,18 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
             }
         }
     }
-    if (P.fa) {
+    if (P.fa && P.fa->kind == 2 && (!tensor_map_encoder() || P.nx > 32767)) P.fa = nullptr;
+    free_queue(P);
+    if (P.fa && P.fa->kind == 2) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, P.fa->kfwd, P.fa->nt, P.fa->smem);
+        P.occ_fa = std::max(occ, 1);
+        P.k_fa = 1;
+        P.split_a = false;
+        P.grid_fa = P.occ_fa * sms;
+        const int rq = setup_queue(P);
+        if (rq != GPUFFT_SUCCESS) return rq;
+    } else if (P.fa) {
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, P.fa->kfwd, P.fa->nt, P.fa->smem);
         P.occ_fa = std::max(occ, 1);
@@ -501,6 +622,10 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
                     for (int k : {k0 / 2, k0 / 4, k0 == 8 ? 16 : 0})
                         if (k >= 2) ks[nk++] = k;
                     ks[nk++] = -1;
+                } else if (P->fa && P->fa->kind == 2) {
+                    // the queue form: planes between a plane's two phases (default 8)
+                    ks[nk++] = 4;
+                    ks[nk++] = 16;
                 }
             }
             for (int ki = 0; ki < nk; ++ki) {
@@ -510,7 +635,7 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
                 else
                     setup_fast(*P, best[0], c);
                 if ((pass == 0 && c >= 0 && !P->fa) || (pass == 1 && c >= 0 && !P->fb)) continue;
-                if (pass == 0 && ks[ki] > 0 && P->k_fa != ks[ki]) continue;
+                if (pass == 0 && ks[ki] > 0 && P->fa && P->fa->kind != 2 && P->k_fa != ks[ki]) continue;
                 if (pass == 0 && ks[ki] == -1 && !P->split_a) continue;
                 const float ms = time_pass(*P, buf, s, pass, reps);
                 if (ms < best_ms) {
@@ -707,6 +832,7 @@ int plan_destroy(Plan *P) {
         if (cur != P->device) cudaSetDevice(P->device);
         cudaFree(P->tw_dev);
         if (P->stage_dev) cudaFree(P->stage_dev);
+        free_queue(*P);
         if (cur != P->device && cur >= 0) cudaSetDevice(cur);
     }
     delete P;
@@ -734,6 +860,34 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
         kf = P.fa->kfwd_x;
         ki = P.fa->kinv_x;
     }
+    if (P.fa && P.fa->kind == 2 && !xch && ((uintptr_t)data) % 16 == 0) {
+        // queue-scheduled Pass A: the tensor maps carry this call's field address
+        const long long nh = P.nz / 2 + 1, lines = P.nx * P.ny / 2;
+        const int wy = P.fa->wy, bh = (int)(P.ny / 2);
+        CUtensorMap tm[3];
+        if (!encode_pair_map(&tm[0], data, nh, lines, wy, bh) || !encode_pair_map(&tm[1], data, nh, lines, wy + 2, bh) ||
+            !encode_pair_map(&tm[2], data, nh, lines, 2, bh))
+            return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass A field view");
+        q::PassAQParams qp{};
+        qp.data = data;
+        qp.unp = P.q_unp;
+        qp.stz = P.pa.stz;
+        qp.sty = P.pa.sty;
+        qp.items = fwd ? P.q_items_f : P.q_items_i;
+        qp.nitems = P.q_nitems;
+        qp.ctr = reinterpret_cast<int *>(P.q_dev);
+        qp.need = fwd ? P.q_need : (int)((P.nz / 2) / wy);
+        qp.wait_ns = 2000000000LL;  // 2 s: far above any launch's length
+        if (const char *ev = std::getenv("GPUFFT_QUEUE_WAIT_MS")) qp.wait_ns = 1000000LL * std::max(1, std::atoi(ev));
+        void *args[] = {&qp, &tm[0], &tm[1], &tm[2]};
+        const cudaError_t e =
+            cudaLaunchKernel(fwd ? P.fa->kfwd : P.fa->kinv, dim3(P.grid_fa), dim3(P.fa->nt), args, P.fa->smem, s);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass A (queue)");
+    }
+    if (P.fa && P.fa->kind == 2) {
+        // (a field not 16-byte aligned: the generic kernels below)
+        kf = ki = nullptr;
+    }
     if (P.fa && P.split_a) {
         // forward: z rows then y columns; inverse: y columns then z rows
         prm.K = P.k_fa;
@@ -745,7 +899,7 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
         }
         return GPUFFT_SUCCESS;
     }
-    if (P.fa) {
+    if (P.fa && kf) {
         prm.K = P.k_fa;
         prm.phases = 0;
         cudaLaunchConfig_t cfg = {};
@@ -900,9 +1054,10 @@ int plan_describe(const Plan *P, char *buf, int len) {
              P->pb.wx, P->pb.ntiles);
     s += b;
     if (P->fa) {
-        snprintf(b, sizeof(b), " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu split=%d}",
+        snprintf(b, sizeof(b),
+                 " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu split=%d depth=%d}",
                  P->fa->kind, P->fa->ny, P->fa->m, P->fa->rw, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa,
-                 P->fa->smem, P->split_a ? 1 : 0);
+                 P->fa->smem, P->split_a ? 1 : 0, P->fa->kind == 2 ? P->q_depth : 0);
         s += b;
     }
     if (P->fb) {

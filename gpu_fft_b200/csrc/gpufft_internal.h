@@ -32,6 +32,14 @@ struct Plan {
     bool split_a = false;      // specialised Pass A runs as two launches (kfix == -1)
     bool tc_split = false;     // x pass on the tensor-core radix-16 kernels (GPUFFT_PLAN_TC_SPLIT)
     bool tuned = false;
+    // queue-scheduled Pass A (kind 2, fft_queue.cuh): counters, the forward and
+    // inverse item lists and the full unpack table in one allocation
+    void *q_dev = nullptr;
+    int q_depth = 0;     // planes between a plane's first and second phase in the lists
+    int q_nitems = 0;    // items per launch
+    int q_need = 0;      // first-phase items per plane (forward)
+    const int *q_items_f = nullptr, *q_items_i = nullptr;
+    const void *q_unp = nullptr;
 };
 
 int set_error(int code, const char *fmt, ...);

@@ -12,16 +12,18 @@
 //  * every axis length must be at most kNoAllocMaxAxis (4096); the array holds
 //    the three tables, 3 * 4096 complex doubles = 192 KiB, on every GPU that
 //    loads the library, until the process exits;
-//  * each call overwrites the array with its own tables (asynchronously, on the
-//    caller's stream); calls that overlap on the GPU — on different streams, or
-//    on different host threads — race on it and must be serialised by the caller;
+//  * each call overwrites the array with its own tables: a small kernel on the
+//    caller's stream computes them in FP64 (sincospi) and rounds them once, so
+//    the call copies nothing from the host and is ordered on that stream like
+//    the two passes that follow; calls that overlap on the GPU — on different
+//    streams, or on different host threads — race on the array and must be
+//    serialised by the caller;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current); make
 //    that first call before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -76,15 +78,17 @@ void fill_axis_noalloc(AxisPlan &ax, int n, const std::vector<int> &radices, int
     }
 }
 
-// exp(-2 pi i e / L), e < L, in long double, rounded once; appended to `out`
+// The x, y and z tables back to back: entry e of the table of length L is
+// exp(-2 pi i e / L), computed in FP64 and rounded once to T.
 template <typename T>
-void append_twiddles(std::vector<T> &out, int L) {
-    const long double two_pi = 6.283185307179586476925286766559005768L;
-    for (int e = 0; e < L; ++e) {
-        const long double ang = two_pi * (long double)e / (long double)L;
-        out.push_back((T)cosl(ang));
-        out.push_back((T)(-sinl(ang)));
-    }
+__global__ void noalloc_tables(cx_t<T> *tab, int nx, int ny, int nz) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nx + ny + nz) return;
+    const int L = q < nx ? nx : (q < nx + ny ? ny : nz);
+    const int e = q < nx ? q : (q < nx + ny ? q - nx : q - nx - ny);
+    double sn, cs;
+    sincospi(2.0 * (double)e / (double)L, &sn, &cs);
+    tab[q] = cx_t<T>{(T)cs, (T)(-sn)};
 }
 
 template <typename T>
@@ -115,16 +119,13 @@ int exec_noalloc(int nx, int ny, int nz, bool forward, void *data, cudaStream_t 
     if ((long long)(nx + 2LL * nx * wx) * vs > budget || bytes_a(wz) > budget)
         return set_error(GPUFFT_ERR_UNSUPPORTED, "axis too long for one shared-memory tile");
 
-    // tables into the static array: x, y, z back to back
-    std::vector<T> tab;
-    tab.reserve(2 * (size_t)(nx + ny + nz));
-    append_twiddles<T>(tab, nx);
-    append_twiddles<T>(tab, ny);
-    append_twiddles<T>(tab, nz);
-    const size_t bytes = tab.size() * sizeof(T);
+    // tables into the static array: x, y, z back to back, computed on the stream
+    const size_t bytes = (size_t)(nx + ny + nz) * vs;
     if (bytes > kNoAllocScratchBytes) return set_error(GPUFFT_ERR_UNSUPPORTED, "tables exceed the static scratch");
-    cudaError_t e = cudaMemcpyAsync(scratch, tab.data(), bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "table upload: %s", cudaGetErrorString(e));
+    const int nt = nx + ny + nz;
+    noalloc_tables<T><<<(nt + 255) / 256, 256, 0, s>>>(reinterpret_cast<V *>(scratch), nx, ny, nz);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "table kernel: %s", cudaGetErrorString(e));
     char *base = (char *)scratch;
 
     PassAParams A;

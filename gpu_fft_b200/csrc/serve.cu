@@ -82,9 +82,10 @@ struct Server {
     bool dispatcher_alive = false;
     std::thread thread;
 
-    // plan cache, under mu.  FP32 / FP64 plans only read their tables while
-    // executing, so one plan serves every stream (slot key -1); a 16-bit plan
-    // keeps per-pencil maxima in plan-owned scratch, so each slot has its own.
+    // plan cache, under mu, one plan per (grid, precision, slot): a plan's
+    // executions must not overlap on the GPU (an FP32 plan may hold the work
+    // counters of the queue-scheduled Pass A, a 16-bit plan its per-pencil
+    // maxima), and each slot is one stream.
     std::map<std::tuple<int64_t, int64_t, int64_t, int, int>, void *> plans;
     int64_t head_id = 0;    // oldest queued request and how often later ones passed it
     int head_passed = 0;
@@ -117,7 +118,7 @@ static constexpr size_t kLatencyWindow = 1 << 20;
 
 // plan for a request on a slot (created on first use, then kept); under mu
 static int plan_for(Server &S, const gpufft_request &r, int slot, void **out) {
-    const auto key = std::make_tuple(r.nx, r.ny, r.nz, r.precision, is16(r.precision) ? slot : -1);
+    const auto key = std::make_tuple(r.nx, r.ny, r.nz, r.precision, slot);
     auto it = S.plans.find(key);
     if (it != S.plans.end()) {
         *out = it->second;
@@ -347,8 +348,12 @@ extern "C" int gpufft_server_create(gpufft_server *server, int64_t budget_bytes,
             cudaError_t e = cudaStreamCreateWithFlags(&S->streams[i], cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->events[i], cudaEventDisableTiming);
             if (e != cudaSuccess) {
-                S->streams.resize(i);
-                S->events.resize(i);
+                // destroy what was created before this one failed
+                if (S->streams[i]) cudaStreamDestroy(S->streams[i]);
+                for (int j = 0; j < i; ++j) {
+                    cudaEventDestroy(S->events[j]);
+                    cudaStreamDestroy(S->streams[j]);
+                }
                 delete S;
                 return set_error(GPUFFT_ERR_CUDA, "server streams: %s", cudaGetErrorString(e));
             }
@@ -370,12 +375,15 @@ extern "C" int gpufft_server_prepare(gpufft_server server, const gpufft_request 
     if (request_bytes(*r) < 0) return set_error(GPUFFT_ERR_INVALID, "bad request precision");
     if (S->dryrun) return GPUFFT_SUCCESS;
     std::lock_guard<std::mutex> lk(S->mu);
+    // plans are built on the server's device, whatever the caller's current one
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != S->device) cudaSetDevice(S->device);
     void *p = nullptr;
-    for (int slot = 0; slot < (is16(r->precision) ? S->nslots : 1); ++slot) {
-        const int rc = plan_for(*S, *r, slot, &p);
-        if (rc != GPUFFT_SUCCESS) return rc;
-    }
-    return GPUFFT_SUCCESS;
+    int rc = GPUFFT_SUCCESS;
+    for (int slot = 0; slot < S->nslots && rc == GPUFFT_SUCCESS; ++slot) rc = plan_for(*S, *r, slot, &p);
+    if (cur != S->device && cur >= 0) cudaSetDevice(cur);
+    return rc;
 }
 
 extern "C" int gpufft_server_submit(gpufft_server server, const gpufft_request *r, int64_t *id) {
@@ -443,6 +451,20 @@ extern "C" int gpufft_server_wait(gpufft_server server, int64_t id, double timeo
     return set_error(q.rc ? q.rc : GPUFFT_ERR_CUDA, "request %lld failed: %s", (long long)id, q.msg.c_str());
 }
 
+extern "C" int gpufft_server_release(gpufft_server server, int64_t id) {
+    Server *S = reinterpret_cast<Server *>(server);
+    if (!S) return set_error(GPUFFT_ERR_INVALID, "no server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return set_error(GPUFFT_ERR_INVALID, "unknown request %lld", (long long)id);
+    const int st = it->second.status;
+    if (st == GPUFFT_REQ_QUEUED || st == GPUFFT_REQ_RUNNING)
+        return set_error(GPUFFT_ERR_INVALID, "request %lld is still %s", (long long)id,
+                         st == GPUFFT_REQ_QUEUED ? "queued" : "running");
+    S->reqs.erase(it);
+    return GPUFFT_SUCCESS;
+}
+
 extern "C" int gpufft_server_cancel(gpufft_server server, int64_t id) {
     Server *S = reinterpret_cast<Server *>(server);
     if (!S) return set_error(GPUFFT_ERR_INVALID, "no server");
@@ -476,6 +498,7 @@ extern "C" int gpufft_server_stats(gpufft_server server, gpufft_server_stats_t *
     st->p50_ms = pct(50);
     st->p99_ms = pct(99);
     st->plans = (int64_t)S->plans.size();
+    st->records = (int64_t)S->reqs.size();
     return GPUFFT_SUCCESS;
 }
 

@@ -150,9 +150,10 @@ int gpufft_wisdom_load(const char *path);
  * Its twiddle tables live in a static device array of 192 KiB that every GPU
  * loading the library holds until exit; every axis must be at most 4096
  * (larger grids are rejected with GPUFFT_ERR_UNSUPPORTED).  Every call
- * rewrites that array, so calls that overlap on the GPU race: serialise
- * them.  The first call on each device looks up the array's address; make
- * that first call before any stream capture. */
+ * rewrites that array with a small kernel on `stream` (nothing is copied
+ * from the host), so calls that overlap on the GPU race: serialise them.
+ * The first call on each device looks up the array's address; make that
+ * first call before any stream capture. */
 int gpufft_exec_noalloc(int64_t nx, int64_t ny, int64_t nz, int dtype, int forward, void *data, void *stream);
 
 /* --------------------------------------------------------------------------
@@ -300,6 +301,7 @@ typedef struct {
     int64_t completed, failed, cancelled, queued, in_flight, max_in_flight;
     int64_t bytes_in_use, peak_bytes_in_use, plans;
     double p50_ms, p99_ms;
+    int64_t records; /* request records held: submitted and not yet released */
 } gpufft_server_stats_t;
 typedef struct gpufft_server_s *gpufft_server;
 #define GPUFFT_SERVER_DRYRUN 1 /* host timers instead of the GPU (tests of the scheduling) */
@@ -310,12 +312,22 @@ int gpufft_server_create(gpufft_server *server, int64_t budget_bytes, int slots,
 /* Stops admitting, lets requests in flight finish, fails those still queued. */
 int gpufft_server_stop(gpufft_server server);
 int gpufft_server_destroy(gpufft_server server);
-/* Builds the plan a request of this shape and precision will use. */
+/* Builds the plans (one per slot) a request of this shape and precision will
+ * use, on the server's device. */
 int gpufft_server_prepare(gpufft_server server, const gpufft_request *request);
+/* Every submitted request keeps a record (status, latency) until it is
+ * released: by gpufft_server_wait once the wait reports its final status, or
+ * by gpufft_server_release.  Clients that only poll, or cancel and never
+ * wait, release their requests explicitly, or the records accumulate. */
 int gpufft_server_submit(gpufft_server server, const gpufft_request *request, int64_t *id);
+/* Status and latency; does not release the record. */
 int gpufft_server_poll(gpufft_server server, int64_t id, int *status, double *latency_ms);
-/* Bounded wait: GPUFFT_ERR_TIMEOUT after timeout_s seconds. */
+/* Bounded wait: GPUFFT_ERR_TIMEOUT after timeout_s seconds.  Releases the
+ * record when it returns a final status. */
 int gpufft_server_wait(gpufft_server server, int64_t id, double timeout_s, double *latency_ms);
+/* Releases the record of a request in a final status (done, failed,
+ * cancelled); GPUFFT_ERR_INVALID while it is queued or running. */
+int gpufft_server_release(gpufft_server server, int64_t id);
 int gpufft_server_cancel(gpufft_server server, int64_t id);
 int gpufft_server_stats(gpufft_server server, gpufft_server_stats_t *stats);
 

@@ -161,6 +161,39 @@ def test_wait_releases_record_and_poll_reports():
     srv.close()
 
 
+def test_poll_only_clients_release_their_records():
+    """Poll does not release a request's record; release does, once the
+    request is final, so a poll-only client leaves nothing behind."""
+    srv = g.Server(budget_bytes=64 * GIB, slots=2, dryrun=True)
+    ids = [srv.submit(srv.request((32, 32, 32), "f32")) for _ in range(20)]
+    cancelled = srv.submit(srv.request(gib_grid(1), "f32"))
+    assert srv.stats()["records"] == 21
+    deadline = time.perf_counter() + 10
+    for rid in ids:
+        while srv.poll(rid)[0] != "done" and time.perf_counter() < deadline:
+            time.sleep(0.001)
+        assert srv.poll(rid)[0] == "done"
+    try:
+        srv.cancel(cancelled)
+    except g.GpuFFTError:
+        pass  # already admitted: it completes instead
+    while srv.poll(cancelled)[0] in ("queued", "running") and time.perf_counter() < deadline:
+        time.sleep(0.001)
+    assert srv.stats()["records"] == 21  # polling keeps them
+    for rid in ids + [cancelled]:
+        srv.release(rid)
+    assert srv.stats()["records"] == 0
+    with pytest.raises(g.GpuFFTError, match="ERR_INVALID"):
+        srv.poll(ids[0])
+    running = srv.submit(srv.request(gib_grid(30), "f32"))
+    wait_running(srv, running)
+    with pytest.raises(g.GpuFFTError, match="ERR_INVALID"):
+        srv.release(running)  # still running
+    srv.wait(running)
+    assert srv.stats()["records"] == 0
+    srv.close()
+
+
 def test_many_clients_threads():
     import threading
 
