@@ -172,28 +172,34 @@ def test_full_size_512_properties(cuda, dt):
     assert spec.abs().max().item() / (n ** 3 / 2) < (1e-5 if dt == "float" else 1e-12)
 
 
+@pytest.mark.parametrize("dt", ["float", "double"])
 @pytest.mark.parametrize("grid", [(1024, 512, 256), (384, 360, 480)], ids=str)
-def test_benchmark_grids_round_trip_and_sampled_parity(oracle, cuda, grid):
-    """The non-cubic and mixed-radix benchmark grids: round trip at full size, and
-    exact parity on a few x-pencils of the spectrum computed by the oracle from
-    the field's plane transforms."""
+def test_benchmark_grids_against_oracle(oracle, cuda, grid, dt):
+    """The non-cubic and mixed-radix benchmark grids, FP32 and FP64, against the
+    FP64 C oracle on every output of R2C and of C2R, and the round trip."""
     import torch
     import gpu_fft_b200 as g
 
     nx, ny, nz = grid
-    f = oracle.normal_field(nx, ny, nz, seed=4, dtype=np.float32)
-    p = g.Plan(nx, ny, nz, "float")
+    f = oracle.normal_field(nx, ny, nz, seed=4, dtype=NPDT[dt])
+    p = g.Plan(nx, ny, nz, dt)
     d = torch.from_numpy(f).cuda()
     p.r2c(d)
     torch.cuda.synchronize()
-    spec = d.cpu().numpy().view(np.complex64).reshape(nx, ny, nz // 2 + 1)
+    cdt = np.complex64 if dt == "float" else np.complex128
+    spec = d.cpu().numpy().view(cdt).reshape(nx, ny, nz // 2 + 1)
     # oracle on the full grid (FP64, all host threads)
     want = oracle.c_r2c(f.astype(np.float64), nx, ny, nz, steps=False)
-    assert oracle.rel_l2(spec, want) < TOL["float"]
+    assert oracle.rel_l2(spec, want) < TOL[dt]
     p.c2r(d)
     torch.cuda.synchronize()
     back = d.cpu().numpy()
-    assert np.max(np.abs(back[:, :, :nz] / (nx * ny * nz) - f[:, :, :nz])) < 2e-5
+    assert np.max(np.abs(back[:, :, :nz] / (nx * ny * nz) - f[:, :, :nz])) < (2e-5 if dt == "float" else 1e-12)
+    del spec, back
+    # C2R of the exact spectrum against the oracle's C2R
+    got = run_c2r(want, grid, dt, plan=p)
+    want_back = oracle.c_c2r(want, nx, ny, nz, steps=False)
+    assert oracle.rel_l2(got[:, :, :nz], want_back[:, :, :nz]) < TOL[dt]
 
 
 def test_deterministic_and_stream_ordered(oracle, cuda):

@@ -60,6 +60,77 @@ def test_16bit_spectrum_close_to_fp32_path(cuda):
     assert err < BAR["fp16"], err
 
 
+def _turbulence(n, seed):
+    """k^-5/3 isotropic random-phase field on 1 <= |k| <= n/3, zero above,
+    made real by this library's FP64 C2R (itself oracle-pinned) and scaled to
+    unit RMS: the precision configuration's input.  float64 padded field."""
+    import math
+
+    import torch
+    import gpu_fft_b200 as g
+
+    nh = n // 2 + 1
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    k = torch.arange(n, device="cuda", dtype=torch.float64)
+    k = torch.where(k <= n // 2, k, k - n)
+    kz = torch.arange(nh, device="cuda", dtype=torch.float64)
+    buf = torch.empty((n, n, nh, 2), dtype=torch.float64, device="cuda")
+    for x in range(0, n, 64):
+        kk = torch.sqrt(k[x:x + 64, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2)
+        kc = kk.clamp(min=1)
+        amp = torch.where((kk >= 1) & (kk <= n / 3.0), torch.sqrt(kc ** (-5.0 / 3.0) / (4 * math.pi * kc ** 2)),
+                          torch.zeros_like(kk))
+        ph = torch.rand(kk.shape, generator=gen, device="cuda", dtype=torch.float64) * (2 * math.pi)
+        buf[x:x + 64, :, :, 0] = amp * torch.cos(ph)
+        buf[x:x + 64, :, :, 1] = amp * torch.sin(ph)
+        del kk, kc, amp, ph
+    field = buf.view(n, n, 2 * nh)
+    p64 = g.Plan(n, n, n, "double")
+    p64.c2r(field)
+    field /= torch.sqrt((field[:, :, :n] ** 2).mean())
+    field[:, :, n:] = 0
+    return field, p64
+
+
+# measured on B200 (1024^3): FP16 3.4e-4, BF16 2.6e-3; the bars are the
+# precision form's stated ones (FP16 1e-3; BF16, one rounding of which is
+# already 1.7e-3, 6e-3)
+@pytest.mark.parametrize("n", [512, 1024])
+def test_16bit_benchmark_sizes_against_fp64_plan(cuda, n):
+    """The 16-bit kernels the precision configuration is quoted on (512^3 and
+    1024^3), on its turbulence field, against this library's FP64 R2C of the
+    same field; then C2R back to N^3 f."""
+    import torch
+    import gpu_fft_b200 as g
+
+    f64, p64 = _turbulence(n, seed=2025)
+    ref = f64.clone()
+    p64.r2c(ref)
+    del p64
+    refc = ref.view(n, n, n // 2 + 1, 2)
+    ref_norm = refc.norm().item()
+    for fmt in ("fp16", "bf16"):
+        p = g.Plan16(n, n, n, fmt)
+        field, scales = p.empty()
+        p.quantize(f64.float(), field, scales)
+        p.r2c(field, scales)
+        spec = torch.empty((n, n, n // 2 + 1, 2), dtype=torch.float32, device="cuda")
+        p.dequantize(field, scales, spec, spectrum=True)
+        err = ((spec.double() - refc).norm() / ref_norm).item()
+        del spec
+        assert err < BAR[fmt], (fmt, n, err)
+        p.c2r(field, scales)
+        real = torch.empty((n, n, n + 2), dtype=torch.float32, device="cuda")
+        p.dequantize(field, scales, real, spectrum=False)
+        back = real[:, :, :n].double() / n ** 3
+        del real
+        err_b = ((back - f64[:, :, :n]).norm() / f64[:, :, :n].norm()).item()
+        del back
+        assert err_b < 2 * BAR[fmt], (fmt, n, err_b)
+        del p, field, scales
+        torch.cuda.synchronize()
+
+
 def test_16bit_rejects_grids_without_kernels(cuda):
     import gpu_fft_b200 as g
 
