@@ -48,6 +48,14 @@ NX = NY = NZ = 512
 DTYPE = "float"
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, by (grid, dtype),
+# kernel and the plan-description fragments of the captured configuration
+NCU_TRAFFIC = {
+    ((512, 512, 512, "float"), "pass_A_fwd",
+     ("fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4 ", "split=0}")): 560_384_512 + 771_755_008,
+}
+
+
 def field_bytes(nx, ny, nz, dt):
     return nx * ny * (nz // 2 + 1) * (8 if dt == "float" else 16)
 
@@ -305,16 +313,17 @@ def run_ours(args, world, rank):
     dom = max(kmean, key=kmean.get)
     peak, peak_kind = load_peaks()
     achieved = 2 * S / (kmean[dom] * 1e-3) / 1e9
-    # DRAM bytes (read + write) per launch of the dominant kernel from the ncu
-    # capture summarised in profiles/pass_a_fast_512cubed_f32.md; reported
-    # only when this run uses the same kernel configuration
-    traffic = None
-    if (nx, ny, nz, dt) == (512, 512, 512, "float") and dom == "pass_A_fwd" and \
-            "fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4 " in plan.describe() and \
-            "split=0}" in plan.describe():
-        traffic = 560_384_512 + 771_755_008
+    # DRAM bytes (read + write) per launch of the dominant kernel: a constant
+    # from one ncu capture of the same kernel configuration on this grid,
+    # reported only when this run's plan uses that configuration
+    traffic, traffic_src = None, None
+    desc = plan.describe()
+    for (grid_dt, kern, conf), nbytes in NCU_TRAFFIC.items():
+        if grid_dt == (nx, ny, nz, dt) and kern == dom and all(c in desc for c in conf):
+            traffic = nbytes
+            traffic_src = "constant from an ncu capture of this kernel configuration (not measured in this run)"
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src, "kernel": dom,
                 "algorithmic_bytes_per_launch": 2 * S, "peak_source": peak_kind,
                 "kernel_ms": {k: round(v, 4) for k, v in kmean.items()}}
     step_bytes = 8 * S  # 2 transforms x (2 passes x (read + write) of S)

@@ -14,7 +14,12 @@
 // per transform, release/acquire at GPU scope).  All first-pass items are
 // taken before any second-pass item and nothing waits inside the first
 // pass, so every wait ends; the wait is still bounded (about two seconds),
-// after which the kernel records an error and skips the item.
+// after which the kernel records an error and skips the item, and the other
+// waits of the launch give up at once.  Two environment variables read when
+// a batch is created exist for tests of that path: GPUFFT_BATCH_WAIT_SPINS
+// (the spin limit, ~500 ns per spin) and GPUFFT_BATCH_UNREACHABLE=t (transform
+// t's second pass waits for one first-pass item more than exist, so its
+// wait always runs out).
 //
 // The items run the size-generic device code of fft_kernels.cuh with each
 // transform's own radix plan and twiddle tables, so one kernel serves any mix
@@ -32,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -117,7 +123,7 @@ __device__ void batch_tile(const BatchDesc &D, long long tile, unsigned char *sm
 template <typename T>
 __global__ void __launch_bounds__(kThreads) batch_kernel(const BatchDesc *__restrict__ descs,
                                                          const BatchItem *__restrict__ items, int nitems,
-                                                         BatchScratch *scratch) {
+                                                         BatchScratch *scratch, long long wait_spins) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
     __shared__ int s_skip;
@@ -132,11 +138,12 @@ __global__ void __launch_bounds__(kThreads) batch_kernel(const BatchDesc *__rest
         if (item.second) {
             if (threadIdx.x == 0) {
                 int skip = 1;
-                for (long long spin = 0; spin < kBatchWaitSpins; ++spin) {
+                for (long long spin = 0; spin < wait_spins; ++spin) {
                     if (ld_acquire(&scratch->done[item.t]) >= D.n_first) {
                         skip = 0;
                         break;
                     }
+                    if (ld_acquire(&scratch->err) != 0) break;  // another wait gave up: so does this one
                     __nanosleep(500);
                 }
                 if (skip) atomicExch(&scratch->err, 1);
@@ -179,6 +186,7 @@ struct Batch {
     size_t scratch_bytes = 0;
     size_t smem = 0;
     int grid = 0;
+    long long wait_spins = kBatchWaitSpins;
     // captured launch (scratch memset + kernel); replayed by gpufft_batch_exec_graph
     cudaGraphExec_t gexec = nullptr;
     bool gready = false;
@@ -246,6 +254,12 @@ static int batch_configure(Batch &B) {
             }
             if (round == 0 && pass == 1 && P.nx == 1) B.hdesc[t].n_first = 0;  // nothing to wait for
         }
+    // test hooks of the bounded wait (header comment)
+    if (const char *ev = std::getenv("GPUFFT_BATCH_WAIT_SPINS")) B.wait_spins = std::max(1LL, std::atoll(ev));
+    if (const char *ev = std::getenv("GPUFFT_BATCH_UNREACHABLE")) {
+        const int t = std::atoi(ev);
+        if (t >= 0 && t < B.n) B.hdesc[t].n_first += 1;
+    }
     B.smem = smem_elems * sizeof(V);
     cudaError_t e = raise_smem_limit((const void *)batch_kernel<T>, B.smem);
     if (e != cudaSuccess)
@@ -382,9 +396,9 @@ static int batch_launch(Batch &B, cudaStream_t s) {
     if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "batch scratch clear: %s", cudaGetErrorString(e));
     const int nitems = (int)B.hitems.size();
     if (B.dtype == GPUFFT_FLOAT)
-        batch_kernel<float><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch);
+        batch_kernel<float><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch, B.wait_spins);
     else
-        batch_kernel<double><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch);
+        batch_kernel<double><<<B.grid, kThreads, B.smem, s>>>(B.ddesc, B.ditems, nitems, B.dscratch, B.wait_spins);
     e = cudaGetLastError();
     return e == cudaSuccess ? GPUFFT_SUCCESS : set_error(GPUFFT_ERR_CUDA, "batch launch: %s", cudaGetErrorString(e));
 }

@@ -1055,9 +1055,9 @@ int plan_describe(const Plan *P, char *buf, int len) {
     s += b;
     if (P->fa) {
         snprintf(b, sizeof(b),
-                 " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu split=%d depth=%d}",
+                 " fastA{kind=%d ny=%d m=%d rw=%d wy=%d nt=%d K=%d grid=%d occ=%d smem=%zu depth=%d split=%d}",
                  P->fa->kind, P->fa->ny, P->fa->m, P->fa->rw, P->fa->wy, P->fa->nt, P->k_fa, P->grid_fa, P->occ_fa,
-                 P->fa->smem, P->split_a ? 1 : 0, P->fa->kind == 2 ? P->q_depth : 0);
+                 P->fa->smem, P->fa->kind == 2 ? P->q_depth : 0, P->split_a ? 1 : 0);
         s += b;
     }
     if (P->fb) {

@@ -167,3 +167,43 @@ def test_batch_schedule_arguments_are_checked(cuda):
     s, b = ctypes.c_int(), ctypes.c_int()
     assert lib.gpufft_batch_schedule(batch._h, ctypes.byref(s), ctypes.byref(b)) == 0
     assert s.value == g.GPUFFT_BATCH_PERSISTENT
+
+
+def test_bounded_wait_runs_out_and_reports(cuda, monkeypatch):
+    """The persistent launch's dependency wait is bounded.  Transform 0's
+    second pass is made to wait for one first-pass item more than exist (a
+    count nothing reaches) with a limit of about a millisecond: the launch
+    ends, gpufft_batch_status reports ERR_CUDA within a second, and the device
+    stays usable -- a batch created afterwards gives the plans' results."""
+    import time
+
+    import torch
+    import gpu_fft_b200 as g
+
+    grids = [(64, 64, 64), (32, 24, 20)]
+    dirs = ["r2c", "c2r"]
+    monkeypatch.setenv("GPUFFT_BATCH_WAIT_SPINS", "2000")
+    monkeypatch.setenv("GPUFFT_BATCH_UNREACHABLE", "0")
+    stalled = g.Batch(grids, dirs, "float", schedule="persistent")
+    monkeypatch.delenv("GPUFFT_BATCH_WAIT_SPINS")
+    monkeypatch.delenv("GPUFFT_BATCH_UNREACHABLE")
+    fields = [_field(gr, 40 + i, torch.float32) for i, gr in enumerate(grids)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    stalled.exec([f.clone() for f in fields])
+    with pytest.raises(g.GpuFFTError, match="ERR_CUDA"):
+        stalled.status()
+    assert time.perf_counter() - t0 < 1.0
+    stalled.close()
+    # the context is intact: a normal batch matches the transforms' own plans
+    batch = g.Batch(grids, dirs, "float", schedule="persistent")
+    got = [f.clone() for f in fields]
+    batch.exec(got)
+    batch.status()
+    for f, gr, d, out in zip(fields, grids, dirs, got):
+        want = f.clone()
+        p = g.Plan(*gr, "float")
+        (p.r2c if d == "r2c" else p.c2r)(want)
+        torch.cuda.synchronize()
+        assert _rel(out, want) < TOL, gr
+    batch.close()
