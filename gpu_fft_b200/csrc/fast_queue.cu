@@ -18,5 +18,20 @@ const VariantA kVariantsA_f32q[] = {
 };
 const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[0]);
 
+// Pass B fed by tensor copies: (Nx, consumer threads, radix variant, ring depth)
+#define TB_ENTRY(T, DT, NX, NT, V, NBUF)                                                                          \
+    {3, DT, NX, q::BShape<T, NX, NT, NBUF>::W, NT, V, q::BShape<T, NX, NT, NBUF>::smem_bytes(),                  \
+     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, false>,                                                \
+     (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, false>,                                               \
+     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, true>, (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, true>}
+
+const VariantB kVariantsB_f32q[] = {
+    TB_ENTRY(float, 0, 512, 256, 1, 3),
+    TB_ENTRY(float, 0, 512, 512, 1, 3),
+    TB_ENTRY(float, 0, 512, 256, 0, 3),
+    TB_ENTRY(float, 0, 512, 256, 1, 2),
+};
+const int kNumVariantsB_f32q = sizeof(kVariantsB_f32q) / sizeof(kVariantsB_f32q[0]);
+
 }  // namespace fast
 }  // namespace gpufft

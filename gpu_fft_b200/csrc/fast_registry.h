@@ -27,7 +27,9 @@ struct VariantA {
 
 struct VariantB {
     int kind;  // 0: tiles loaded by the first FFT stage; 1: tiles double-buffered by cp.async;
-               // 2: one tile buffer refilled by cp.async during the last stage
+               // 2: one tile buffer refilled by cp.async during the last stage;
+               // 3: tiles brought in by tensor copies, NBUF-deep ring (fft_queue.cuh;
+               //    nt counts the copy-issuing warp)
     int dtype;
     int nx;
     int w, nt, v;
@@ -47,6 +49,8 @@ extern const VariantB kVariantsB_f32s[];
 extern const int kNumVariantsB_f32s;
 extern const VariantA kVariantsA_f32q[];  // queue-scheduled Pass A (fast_queue.cu)
 extern const int kNumVariantsA_f32q;
+extern const VariantB kVariantsB_f32q[];  // tensor-copy Pass B (fast_queue.cu)
+extern const int kNumVariantsB_f32q;
 extern const VariantA kVariantsA_f64[];
 extern const int kNumVariantsA_f64;
 extern const VariantB kVariantsB_f64[];

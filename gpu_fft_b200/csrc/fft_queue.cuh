@@ -455,5 +455,94 @@ __global__ void __launch_bounds__(NT + 32, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pass B (x C2C over column tiles) fed by tensor copies.
+//
+// Replaces the reference's strided 1D cuFFT C2C along x
+// (GPU_FFT/src/initialize_GPU_FFT/GPU_FFT_init.cu:66-73,89).  A tile is the
+// NX x W block of W consecutive columns c = ky*Nh + kz (W*8 = 128 bytes per
+// row) of all NX rows: a 2D box of the view [NX][Ny*Nh] (row pitch Ny*Nh*8
+// bytes, a multiple of 16; tile starts are 128-byte aligned), landing in the
+// COLS layout the tile FFT reads.  Tiles have no dependencies: CTA b takes
+// tiles b, b + grid, ...; NBUF tiles are in flight, and thread 0 issues the
+// copies of tile k + NBUF as soon as the barrier after tile k's FFT has freed
+// its buffer (no copy-issuing warp, so every warp's registers go to the FFT).
+// ---------------------------------------------------------------------------
+template <typename T, int NX, int NT, int NBUF>
+struct BShape {
+    using V = cx_t<T>;
+    static constexpr int W = 128 / (int)sizeof(V);
+    static constexpr int BOXH = NX > 256 ? 256 : NX;  // rows per tensor copy
+    static constexpr int NBOX = (NX + BOXH - 1) / BOXH;
+    static constexpr int TILE_BYTES = NX * W * (int)sizeof(V);
+    static constexpr int BUF = (TILE_BYTES + 127) / 128 * 128;
+    static constexpr int TAB = ((NX * (int)sizeof(V)) + 127) / 128 * 128;
+    static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + NBUF * 8 + 128; }
+    static_assert(sizeof(V) == 8, "FP32 complex");
+    static_assert(NX % BOXH == 0, "whole boxes");
+};
+
+template <typename T, int NX, int NT, bool FWD, int VARIANT, int NBUF, bool EPI>
+__global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const __grid_constant__ CUtensorMap tm) {
+    using S = BShape<T, NX, NT, NBUF>;
+    using V = cx_t<T>;
+    using FFT = TileFFT<T, NX, S::W, NT, FWD, COLS, VARIANT, fast::BLOCK>;
+    static_assert(!FFT::kTcStage, "the tensor-core stage uses its own swizzled layout");
+    constexpr int W = S::W;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    V *tw = reinterpret_cast<V *>(smem);
+    unsigned char *bufs = smem + S::TAB;
+    uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF);
+    for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
+    auto issue = [&](long long t, int s) {
+        unsigned char *b = bufs + (size_t)s * S::BUF;
+        mbar_arrive_expect_tx(&full[s], (uint32_t)S::TILE_BYTES);
+#pragma unroll
+        for (int bx = 0; bx < S::NBOX; ++bx)
+            tensor_load_2d(b + (size_t)bx * S::BOXH * W * sizeof(V), &tm, (int)(t * W), bx * S::BOXH, &full[s]);
+    };
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NBUF; ++s) mbar_init(&full[s], 1);
+        fence_mbar_init();
+        for (int s = 0; s < NBUF; ++s) {
+            const long long t = blockIdx.x + (long long)s * gridDim.x;
+            if (t < P.ntiles) issue(t, s);
+        }
+    }
+    __syncthreads();
+    const long long ncols = P.ncols;
+    V *base = reinterpret_cast<V *>(P.data);
+    int k = 0;
+    for (long long t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
+        const int s = k % NBUF;
+        const uint32_t ph = (uint32_t)((k / NBUF) & 1);
+        if (!mbar_wait(&full[s], ph, 2000000000LL)) {
+            mbar_wait(&full[s], ph, 2000000000LL);  // nothing is left in flight at exit
+            break;
+        }
+        V *tile = reinterpret_cast<V *>(bufs + (size_t)s * S::BUF);
+        const long long c0 = t * W;
+        const int wv = (int)min((long long)W, ncols - c0);
+        V *g = base + c0;
+        auto dst = [&](int n, int w, V v) {
+            if (w < wv) {
+                if constexpr (EPI)
+                    st_g(g + (long long)n * ncols + w, pass_b_epilogue(P, v, n, c0 + w));
+                else
+                    st_g(g + (long long)n * ncols + w, v);
+            }
+        };
+        FromSmem fs;
+        FFT::run(fs, dst, tile, tw);
+        __syncthreads();  // every read of the tile is done: refill its buffer
+        const long long tn = t + (long long)NBUF * gridDim.x;
+        if (threadIdx.x == 0 && tn < P.ntiles) {
+            fence_proxy_async_shared();
+            issue(tn, s);
+        }
+    }
+}
+
 }  // namespace q
 }  // namespace gpufft

@@ -236,6 +236,7 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
     static const std::vector<fast::VariantB> f32 = [] {
         std::vector<fast::VariantB> v(fast::kVariantsB_f32, fast::kVariantsB_f32 + fast::kNumVariantsB_f32);
         v.insert(v.end(), fast::kVariantsB_f32s, fast::kVariantsB_f32s + fast::kNumVariantsB_f32s);
+        v.insert(v.end(), fast::kVariantsB_f32q, fast::kVariantsB_f32q + fast::kNumVariantsB_f32q);
         return v;
     }();
     static const std::vector<fast::VariantB> f64(fast::kVariantsB_f64, fast::kVariantsB_f64 + fast::kNumVariantsB_f64);
@@ -245,10 +246,12 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
 // A Pass B entry serves this plan: its length, 16-byte tile rows for the
 // cp.async form, and tensor-core stages (v = 2) exactly when the plan asks
 // for them.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 static bool b_eligible(const Plan &P, const fast::VariantB &v) {
     const int m = (int)(P.nz / 2);
     const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
-    return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v == 2) == P.tc_split);
+    return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v == 2) == P.tc_split) &&
+           (v.kind != 3 || tensor_map_encoder());
 }
 
 // ---------------------------------------------------------------------------
@@ -943,7 +946,26 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd, do
     prm.scale = scale;
     prm.dealias = dealias;
     prm.epi = (scale != 1.0 || dealias) ? 1 : 0;
-    if (P.fb && !(P.fb->kind != 0 && ((uintptr_t)data) % 16 != 0)) {
+    if (P.fb && P.fb->kind == 3 && ((uintptr_t)data) % 16 == 0) {
+        // tensor-copy tiles: the map carries this call's field address
+        prm.wx = P.fb->w;
+        prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
+        CUtensorMap tm;
+        const auto enc = tensor_map_encoder();
+        const cuuint64_t dims[2] = {(cuuint64_t)prm.ncols, (cuuint64_t)P.nx};
+        const cuuint64_t strides[1] = {(cuuint64_t)prm.ncols * 8};
+        const cuuint32_t box[2] = {(cuuint32_t)P.fb->w, (cuuint32_t)std::min<int64_t>(P.nx, 256)};
+        const cuuint32_t es[2] = {1, 1};
+        if (!enc || enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, data, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass B field view");
+        void *args[] = {&prm, &tm};
+        const void *k = prm.epi ? (fwd ? P.fb->kfwd_epi : P.fb->kinv_epi) : (fwd ? P.fb->kfwd : P.fb->kinv);
+        const cudaError_t e = cudaLaunchKernel(k, dim3(P.grid_fb), dim3(P.fb->nt), args, P.fb->smem, s);
+        return e == cudaSuccess ? GPUFFT_SUCCESS : cuda_error(e, "launch pass B (tensor copies)");
+    }
+    if (P.fb && P.fb->kind != 3 && !(P.fb->kind != 0 && ((uintptr_t)data) % 16 != 0)) {
         prm.wx = P.fb->w;
         prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
         void *args[] = {&prm};
