@@ -154,12 +154,12 @@ __device__ __forceinline__ void group_sync() {
 // ---------------------------------------------------------------------------
 // shape of one instantiation
 // ---------------------------------------------------------------------------
-template <typename T, int NY, int M, int NT, int NBUF>
+template <typename T, int NY, int M, int NT, int NBUF, int WY_>
 struct QShape {
     using V = cx_t<T>;
     static constexpr int NH = M + 1;
-    static constexpr int WY = 128 / (int)sizeof(V);  // columns per column item (128-byte rows)
-    static constexpr int RI = 32;                    // rows per row item
+    static constexpr int WY = WY_;                   // columns per column item
+    static constexpr int RI = NT / 16;               // rows per row item (two per consumer warp)
     static constexpr int BH = NY / 2;                // row pairs per box
     static constexpr int NRI = NY / RI;
     static constexpr int NCI = M / WY;
@@ -181,7 +181,8 @@ struct QShape {
     static_assert(NY % RI == 0 && NY % 2 == 0 && BH <= 256, "rows per item / box height");
     static_assert(M % WY == 0, "whole column tiles");
     static_assert(M == 256, "the row FFT is 16 x 16");
-    static_assert(NT == 32 * (RI / 2), "two rows per consumer warp");
+    static_assert(NT % 32 == 0 && NT == 16 * RI, "two rows per consumer warp");
+    static_assert(WY % 2 == 0, "16-byte box rows");
 };
 
 // ---------------------------------------------------------------------------
@@ -215,11 +216,11 @@ __device__ __forceinline__ void row256_step2(V (&x)[16], const V *row, int b) {
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
-template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF>
+template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16>
 __global__ void __launch_bounds__(NT + 32, 1)
     pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
                  const __grid_constant__ CUtensorMap tm_x) {
-    using S = QShape<T, NY, M, NT, NBUF>;
+    using S = QShape<T, NY, M, NT, NBUF, WY_>;
     using V = cx_t<T>;
     using ColFFT = TileFFT<T, NY, S::WY, NT, FWD, COLS, VY, GROUP>;
     using ColL = typename ColFFT::L;

@@ -291,7 +291,7 @@ static std::vector<int> queue_items(int nx, int nfirst, int nsecond, int first_t
 static int setup_queue(Plan &P) {
     free_queue(P);
     const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
-    const int ri = 32, wy = P.fa->wy;
+    const int ri = (P.fa->nt - 32) / 16, wy = P.fa->wy;  // two rows per consumer warp
     const int nri = ny / ri, nci = m / wy;
     int depth = P.kfix > 0 ? P.kfix : 8;
     if (const char *ev = std::getenv("GPUFFT_QUEUE_DEPTH")) depth = std::atoi(ev);
