@@ -41,7 +41,7 @@ EXPORTS = (
     "gpufft_server_submit", "gpufft_server_poll", "gpufft_server_wait", "gpufft_server_cancel", "gpufft_server_stats",
     "gpufft_server_release",
     "gpufft_init_dist", "gpufft_dist_unique_id", "gpufft_dplan_create", "gpufft_dplan_destroy", "gpufft_dexec_r2c", "gpufft_dexec_c2r",
-    "gpufft_dplan_layout", "gpufft_dgroup_create", "gpufft_dgroup_exec",
+    "gpufft_dplan_layout", "gpufft_dgroup_create", "gpufft_dgroup_exec", "gpufft_dist_schedule",
 )
 GPUFFT_PLAN_AUTOTUNE = 1
 GPUFFT_PLAN_TC_SPLIT = 2
@@ -140,6 +140,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_dexec_r2c.argtypes = [vp, vp, vp]
     lib.gpufft_dexec_c2r.argtypes = [vp, vp, vp]
     lib.gpufft_dplan_layout.argtypes = [vp, ctypes.POINTER(i64)]
+    lib.gpufft_dist_schedule.argtypes = [i64, i64, i64, ci, ci, ci, ci, ci, ctypes.POINTER(i64), ci]
     lib.gpufft_dgroup_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci, ci]
     lib.gpufft_dgroup_exec.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ci, ci, vp]
     for name in EXPORTS:
@@ -467,6 +468,34 @@ def slab_layout(nx: int, ny: int, nz: int, procs: int, rank: int) -> dict:
     nxl, nyl, nh = nx // procs, ny // procs, nz // 2 + 1
     return {"x0": rank * nxl, "nxl": nxl, "y0": rank * nyl, "nyl": nyl, "real_shape": (nxl, ny, 2 * nh),
             "spectrum_shape": (nx, nyl, nh)}
+
+
+SCHEDULE_FIELDS = ("kind", "peer", "src_buf", "src_off", "src_pitch", "dst_buf", "dst_off", "dst_pitch", "width", "rows")
+SCHEDULE_KINDS = {0: "copy", 1: "send", 2: "recv"}
+
+
+def dist_schedule(nx: int, ny: int, nz: int, dtype="float", procs: int = 1, rank: int = 0, forward: bool = True,
+                  fused: bool = False) -> list:
+    """The exchange schedule the slab plans of `rank` issue (host only): a
+    list of ops, each a dict of SCHEDULE_FIELDS with kind 'copy' (2D copy
+    between the field, buffer 0, and the exchange buffer, buffer 1), 'send' or
+    'recv' (to / from `peer`); offsets, pitches and widths in bytes."""
+    lib = load_library()
+    args = (nx, ny, nz, _dtype_code(dtype), procs, rank, int(forward), int(fused))
+    n = lib.gpufft_dist_schedule(*args, None, 0)
+    if n > 0:
+        _check(n)
+    n = -n
+    buf = (ctypes.c_int64 * (10 * max(n, 1)))()
+    got = lib.gpufft_dist_schedule(*args, buf, n)
+    if got < 0:
+        _check(1)
+    ops = []
+    for i in range(got):
+        rec = dict(zip(SCHEDULE_FIELDS, buf[10 * i:10 * i + 10]))
+        rec["kind"] = SCHEDULE_KINDS[rec["kind"]]
+        ops.append(rec)
+    return ops
 
 
 def dist_unique_id() -> bytes:

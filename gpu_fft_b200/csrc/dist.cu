@@ -107,6 +107,16 @@ int nccl_error(ncclResult_t r, const char *what) {
 
 }  // namespace
 
+// one copy of the exchange schedule (byte offsets and pitches)
+struct XferOp {
+    enum Kind { COPY = 0, SEND = 1, RECV = 2 };
+    enum Buf { FIELD = 0, XBUF = 1 };  // the user's field, the plan's exchange buffer
+    int kind;
+    int peer;  // SEND / RECV: the other rank
+    int src_buf, dst_buf;
+    int64_t src_off, src_pitch, dst_off, dst_pitch, width, rows;
+};
+
 struct DistPlan {
     int64_t nx = 0, ny = 0, nz = 0;
     int dtype = 0, procs = 1, rank = 0, device = 0;
@@ -156,35 +166,91 @@ static int dist_setup(DistPlan *D, int64_t nx, int64_t ny, int64_t nz, int dtype
     return GPUFFT_SUCCESS;
 }
 
-// chunk s of the send buffer = rows [s*nyl, (s+1)*nyl) of every local plane
-static int pack(const DistPlan &D, const void *data, cudaStream_t s) {
-    const size_t w = (size_t)D.nyl * D.nh * D.cs, pitch = (size_t)D.ny * D.nh * D.cs;
-    for (int r = 0; r < D.procs; ++r) {
-        const cudaError_t e = cudaMemcpy2DAsync((char *)D.sendbuf + r * D.chunk, w, (const char *)data + r * w, pitch,
-                                                w, (size_t)D.nxl, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "pack: %s", cudaGetErrorString(e));
+// ---------------------------------------------------------------------------
+// The exchange schedule of one rank: the copies that move its data between
+// the slab layouts, in the order they are issued.  One host function (no
+// device needed) describes them for the NCCL path, the in-process group and
+// gpufft_dist_schedule, so the CPU tests drive the same schedule.
+//   forward: [pack: chunk s of the exchange buffer = rows [s*nyl, (s+1)*nyl)
+//            of every local plane, one 2D copy per s]
+//            then for each peer p: send chunk p of the exchange buffer to p,
+//            receive p's chunk into block p of the field (the y-slab
+//            [X = p*nxl + xl][yl][kz] that Pass B reads);
+//   inverse: for each peer p: send block p of the field to p, receive p's
+//            block into chunk p of the exchange buffer;
+//            then [unpack: chunk s into rows [s*nyl, ...) of every plane].
+// The bracketed copies are left out when Pass A itself writes (forward) or
+// reads (inverse) the exchange buffer's layout (the XCH kernels).
+// ---------------------------------------------------------------------------
+static std::vector<XferOp> dist_schedule(int64_t ny, int64_t nxl, int64_t nyl, int64_t nh, size_t cs, int procs,
+                                         bool fwd, bool packed) {
+    std::vector<XferOp> ops;
+    const int64_t w = nyl * nh * (int64_t)cs, pitch = ny * nh * (int64_t)cs, chunk = nxl * w;
+    auto pack_ops = [&](bool to_buf) {
+        for (int r = 0; r < procs; ++r) {
+            XferOp o{};
+            o.kind = XferOp::COPY;
+            o.peer = -1;
+            o.src_buf = to_buf ? XferOp::FIELD : XferOp::XBUF;
+            o.dst_buf = to_buf ? XferOp::XBUF : XferOp::FIELD;
+            o.src_off = to_buf ? r * w : r * chunk;
+            o.src_pitch = to_buf ? pitch : w;
+            o.dst_off = to_buf ? r * chunk : r * w;
+            o.dst_pitch = to_buf ? w : pitch;
+            o.width = w;
+            o.rows = nxl;
+            ops.push_back(o);
+        }
+    };
+    if (fwd && !packed) pack_ops(true);
+    for (int p = 0; p < procs; ++p) {
+        XferOp snd{}, rcv{};
+        snd.kind = XferOp::SEND;
+        rcv.kind = XferOp::RECV;
+        snd.peer = rcv.peer = p;
+        snd.src_buf = fwd ? XferOp::XBUF : XferOp::FIELD;
+        rcv.dst_buf = fwd ? XferOp::FIELD : XferOp::XBUF;
+        snd.src_off = rcv.dst_off = p * chunk;
+        snd.width = rcv.width = chunk;
+        snd.rows = rcv.rows = 1;
+        snd.src_pitch = snd.dst_pitch = rcv.src_pitch = rcv.dst_pitch = chunk;
+        ops.push_back(snd);
+        ops.push_back(rcv);
+    }
+    if (!fwd && !packed) pack_ops(false);
+    return ops;
+}
+
+static std::vector<XferOp> schedule_of(const DistPlan &D, bool fwd, bool packed) {
+    return dist_schedule(D.ny, D.nxl, D.nyl, D.nh, D.cs, D.procs, fwd, packed);
+}
+
+static char *buf_of(const DistPlan &D, void *data, int which) {
+    return which == XferOp::FIELD ? (char *)data : (char *)D.sendbuf;
+}
+
+// the local copies (pack or unpack) of the schedule
+static int local_copies(const DistPlan &D, void *data, const std::vector<XferOp> &ops, cudaStream_t s) {
+    for (const XferOp &o : ops) {
+        if (o.kind != XferOp::COPY) continue;
+        const cudaError_t e =
+            cudaMemcpy2DAsync(buf_of(D, data, o.dst_buf) + o.dst_off, (size_t)o.dst_pitch, buf_of(D, data, o.src_buf) + o.src_off,
+                              (size_t)o.src_pitch, (size_t)o.width, (size_t)o.rows, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "slab copy: %s", cudaGetErrorString(e));
     }
     return GPUFFT_SUCCESS;
 }
 
-// the inverse of pack: chunk s of the receive buffer into rows [s*nyl, ...) of every plane
-static int unpack(const DistPlan &D, void *data, cudaStream_t s) {
-    const size_t w = (size_t)D.nyl * D.nh * D.cs, pitch = (size_t)D.ny * D.nh * D.cs;
-    for (int r = 0; r < D.procs; ++r) {
-        const cudaError_t e = cudaMemcpy2DAsync((char *)data + r * w, pitch, (const char *)D.sendbuf + r * D.chunk, w,
-                                                w, (size_t)D.nxl, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "unpack: %s", cudaGetErrorString(e));
-    }
-    return GPUFFT_SUCCESS;
-}
-
-// all-to-all over NCCL: chunk s of `from` to rank s, chunk s of `to` from rank s
-static int exchange_nccl(const DistPlan &D, const void *from, void *to, cudaStream_t s) {
+// the sends and receives of the schedule over NCCL, as one group
+static int exchange_nccl(const DistPlan &D, void *data, const std::vector<XferOp> &ops, cudaStream_t s) {
     const Nccl &n = nccl();
     ncclResult_t r = n.groupStart();
-    for (int p = 0; p < D.procs && r == ncclSuccess; ++p) {
-        r = n.send((const char *)from + p * D.chunk, D.chunk, ncclUint8, p, D.comm, s);
-        if (r == ncclSuccess) r = n.recv((char *)to + p * D.chunk, D.chunk, ncclUint8, p, D.comm, s);
+    for (const XferOp &o : ops) {
+        if (r != ncclSuccess) break;
+        if (o.kind == XferOp::SEND)
+            r = n.send(buf_of(D, data, o.src_buf) + o.src_off, (size_t)o.width, ncclUint8, o.peer, D.comm, s);
+        else if (o.kind == XferOp::RECV)
+            r = n.recv(buf_of(D, data, o.dst_buf) + o.dst_off, (size_t)o.width, ncclUint8, o.peer, D.comm, s);
     }
     ncclResult_t g = n.groupEnd();
     if (r != ncclSuccess) return nccl_error(r, "exchange");
@@ -221,22 +287,23 @@ int dist_exec(DistPlan *D, void *data, cudaStream_t s, bool fwd) {
     if (!data) return set_error(GPUFFT_ERR_INVALID, "data pointer is NULL");
     int rc;
     const bool fused = D->comm && fused_xch(*D);
+    const std::vector<XferOp> ops = schedule_of(*D, fwd, fused);
     if (fwd) {
         if (fused) {
             rc = pass_a_xch(*D, data, s, true);
         } else {
             rc = plan_exec_pass(D->pa, data, s, 0, true);
-            if (D->comm && rc == GPUFFT_SUCCESS) rc = pack(*D, data, s);
+            if (D->comm && rc == GPUFFT_SUCCESS) rc = local_copies(*D, data, ops, s);
         }
-        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, D->sendbuf, data, s);
+        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, data, ops, s);
         if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D->pb, data, s, 1, true);
     } else {
         rc = plan_exec_pass(D->pb, data, s, 1, false);
-        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, data, D->sendbuf, s);
+        if (D->comm && rc == GPUFFT_SUCCESS) rc = exchange_nccl(*D, data, ops, s);
         if (fused) {
             if (rc == GPUFFT_SUCCESS) rc = pass_a_xch(*D, data, s, false);
         } else {
-            if (D->comm && rc == GPUFFT_SUCCESS) rc = unpack(*D, data, s);
+            if (D->comm && rc == GPUFFT_SUCCESS) rc = local_copies(*D, data, ops, s);
             if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D->pa, data, s, 0, false);
         }
     }
@@ -338,6 +405,33 @@ extern "C" int gpufft_dplan_layout(gpufft_dplan plan, int64_t *out) {
     return GPUFFT_SUCCESS;
 }
 
+extern "C" int gpufft_dist_schedule(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank, int forward,
+                                    int fused, int64_t *ops, int cap) {
+    if (procs < 1 || rank < 0 || rank >= procs) return set_error(GPUFFT_ERR_INVALID, "rank %d of %d ranks", rank, procs);
+    if (dtype != GPUFFT_FLOAT && dtype != GPUFFT_DOUBLE)
+        return set_error(GPUFFT_ERR_INVALID, "dtype %d is neither GPUFFT_FLOAT nor GPUFFT_DOUBLE", dtype);
+    if (nx < 1 || ny < 1 || nz < 2 || nx % procs || ny % procs)
+        return set_error(GPUFFT_ERR_INVALID, "grid %lldx%lldx%lld: Nx and Ny must be multiples of procs=%d",
+                         (long long)nx, (long long)ny, (long long)nz, procs);
+    const std::vector<XferOp> v = dist_schedule(ny, nx / procs, ny / procs, nz / 2 + 1, dtype == GPUFFT_FLOAT ? 8 : 16,
+                                                procs, forward != 0, fused != 0);
+    if (!ops || cap < (int)v.size()) return -(int)v.size();  // the size needed
+    for (size_t i = 0; i < v.size(); ++i) {
+        int64_t *o = ops + 10 * i;
+        o[0] = v[i].kind;
+        o[1] = v[i].peer;
+        o[2] = v[i].src_buf;
+        o[3] = v[i].src_off;
+        o[4] = v[i].src_pitch;
+        o[5] = v[i].dst_buf;
+        o[6] = v[i].dst_off;
+        o[7] = v[i].dst_pitch;
+        o[8] = v[i].width;
+        o[9] = v[i].rows;
+    }
+    return (int)v.size();
+}
+
 extern "C" int gpufft_dgroup_create(gpufft_dplan *plans, int64_t nx, int64_t ny, int64_t nz, int dtype, int procs) {
     if (!plans || procs < 1) return set_error(GPUFFT_ERR_INVALID, "plans array and procs >= 1 are required");
     for (int r = 0; r < procs; ++r) plans[r] = nullptr;
@@ -368,39 +462,46 @@ extern "C" int gpufft_dgroup_exec(gpufft_dplan *plans, void **data, int procs, i
             return set_error(GPUFFT_ERR_INVALID, "plans[%d] is not rank %d of an in-process group of %d", r, r, procs);
     }
     cudaStream_t s = (cudaStream_t)stream;
-    // all-to-all by device copies: chunk q of rank p's `from` -> chunk p of rank q's `to`
-    auto exchange = [&](bool to_data) -> int {
+    const bool fused = procs > 1 && fused_xch(*D[0]);
+    std::vector<std::vector<XferOp>> ops(procs);
+    for (int r = 0; r < procs; ++r) ops[r] = schedule_of(*D[r], forward != 0, fused);
+    // the schedules' sends and receives matched up as device copies: rank
+    // p's send to q lands where q's receive from p points
+    auto exchange = [&]() -> int {
         for (int p = 0; p < procs; ++p)
-            for (int q = 0; q < procs; ++q) {
-                const char *src = to_data ? (const char *)D[p]->sendbuf : (const char *)data[p];
-                char *dst = to_data ? (char *)data[q] : (char *)D[q]->sendbuf;
-                const cudaError_t e = cudaMemcpyAsync(dst + p * D[p]->chunk, src + q * D[p]->chunk, D[p]->chunk,
-                                                      cudaMemcpyDeviceToDevice, s);
-                if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "group exchange: %s", cudaGetErrorString(e));
+            for (const XferOp &o : ops[p]) {
+                if (o.kind != XferOp::SEND) continue;
+                const int q = o.peer;
+                for (const XferOp &i : ops[q]) {
+                    if (i.kind != XferOp::RECV || i.peer != p) continue;
+                    const cudaError_t e =
+                        cudaMemcpyAsync(buf_of(*D[q], data[q], i.dst_buf) + i.dst_off, buf_of(*D[p], data[p], o.src_buf) + o.src_off,
+                                        (size_t)o.width, cudaMemcpyDeviceToDevice, s);
+                    if (e != cudaSuccess) return set_error(GPUFFT_ERR_CUDA, "group exchange: %s", cudaGetErrorString(e));
+                }
             }
         return GPUFFT_SUCCESS;
     };
     int rc = GPUFFT_SUCCESS;
-    const bool fused = procs > 1 && fused_xch(*D[0]);
     if (forward) {
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) {
             if (fused) {
                 rc = pass_a_xch(*D[r], data[r], s, true);
             } else {
                 rc = plan_exec_pass(D[r]->pa, data[r], s, 0, true);
-                if (rc == GPUFFT_SUCCESS && procs > 1) rc = pack(*D[r], data[r], s);
+                if (rc == GPUFFT_SUCCESS && procs > 1) rc = local_copies(*D[r], data[r], ops[r], s);
             }
         }
-        if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange(true);
+        if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange();
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) rc = plan_exec_pass(D[r]->pb, data[r], s, 1, true);
     } else {
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) rc = plan_exec_pass(D[r]->pb, data[r], s, 1, false);
-        if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange(false);
+        if (rc == GPUFFT_SUCCESS && procs > 1) rc = exchange();
         for (int r = 0; r < procs && rc == GPUFFT_SUCCESS; ++r) {
             if (fused) {
                 rc = pass_a_xch(*D[r], data[r], s, false);
             } else {
-                if (procs > 1) rc = unpack(*D[r], data[r], s);
+                if (procs > 1) rc = local_copies(*D[r], data[r], ops[r], s);
                 if (rc == GPUFFT_SUCCESS) rc = plan_exec_pass(D[r]->pa, data[r], s, 0, false);
             }
         }

@@ -14,13 +14,13 @@ namespace fast {
      (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY>, nullptr, nullptr}
 
 const VariantA kVariantsA_f32q[] = {
-    // 512^2 planes, B200: 16 consumer warps with a 3-deep ring of 72 KB
-    // buffers took 0.400 / 0.426 ms per launch (forward / inverse) at 512^3
-    QA_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
+    // 512^2 planes, B200, ms per launch at 512^3 (forward / inverse, queue
+    // depth 16-32): 16 consumer warps, 16-column items, 3-deep ring of 72 KB
+    // buffers 0.398 / 0.426; 2-deep 0.412 / 0.435.  Measured and dropped:
+    // 8 consumer warps (16-row items) 0.425 / 0.473, 8-column items with a
+    // 4-deep ring 0.475 / 0.520 (8 warps) and 0.457 / 0.500 (16 warps)
     QA_ENTRY(float, 0, 512, 256, 512, 0, 3, 16),
-    QA_ENTRY(float, 0, 512, 256, 256, 0, 3, 16),
-    QA_ENTRY(float, 0, 512, 256, 256, 0, 4, 8),
-    QA_ENTRY(float, 0, 512, 256, 512, 0, 3, 8),
+    QA_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
 };
 const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[0]);
 

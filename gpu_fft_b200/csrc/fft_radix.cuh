@@ -9,6 +9,7 @@
 // The trigonometric constants are the mathematical values written out to
 // 25 significant digits and rounded by the compiler to the storage type.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -21,6 +22,28 @@ template <typename T> using cx_t = typename CxOf<T>::type;
 
 template <typename V> __device__ __forceinline__ V c_add(V a, V b) { return V{a.x + b.x, a.y + b.y}; }
 template <typename V> __device__ __forceinline__ V c_sub(V a, V b) { return V{a.x - b.x, a.y - b.y}; }
+// FP32 complex add / subtract as one packed f32x2 operation (sm_100): the
+// same IEEE sums as the two scalar ones, half the instructions
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+    unsigned long long u;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(u) : "f"(v.x), "f"(v.y));
+    return u;
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long u) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(u));
+    return v;
+}
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return bits_f2(d);
+}
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return bits_f2(d);
+}
 template <typename V> __device__ __forceinline__ V c_mul(V a, V b) {
     return V{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
@@ -182,11 +205,20 @@ template <bool FWD, typename V> __device__ __forceinline__ void dft2(V &a, V &b)
 }
 
 template <bool FWD, typename V> __device__ __forceinline__ void dft4(V &x0, V &x1, V &x2, V &x3) {
-    V t0 = c_add(x0, x2), t1 = c_sub(x0, x2), t2 = c_add(x1, x3), t3 = c_rot<FWD>(c_sub(x1, x3));
+    V t0 = c_add(x0, x2), t1 = c_sub(x0, x2), t2 = c_add(x1, x3);
     x0 = c_add(t0, t2);
     x2 = c_sub(t0, t2);
-    x1 = c_add(t1, t3);
-    x3 = c_sub(t1, t3);
+    if constexpr (std::is_same<V, float2>::value) {
+        // t1 -/+ i d with the rotation folded into scalar adds (a packed add
+        // would first have to build the swapped pair)
+        const V d = c_sub(x1, x3);
+        x1 = FWD ? V{t1.x + d.y, t1.y - d.x} : V{t1.x - d.y, t1.y + d.x};
+        x3 = FWD ? V{t1.x - d.y, t1.y + d.x} : V{t1.x + d.y, t1.y - d.x};
+    } else {
+        const V t3 = c_rot<FWD>(c_sub(x1, x3));
+        x1 = c_add(t1, t3);
+        x3 = c_sub(t1, t3);
+    }
 }
 
 // length-3 DFT in place: y0 = a+b+c, y1,2 = a - (b+c)/2 -/+ i (sqrt3/2)(b-c) (forward)

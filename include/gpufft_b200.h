@@ -270,6 +270,18 @@ int gpufft_dplan_layout(gpufft_dplan plan, int64_t *out);
 /* All `procs` ranks in this process on the current device, exchanging by
  * device copies (no NCCL): the same decomposition on one GPU. */
 int gpufft_dgroup_create(gpufft_dplan *plans, int64_t nx, int64_t ny, int64_t nz, int dtype, int procs);
+/* The exchange schedule of `rank` (replaces the reference's MPI_Isend /
+ * MPI_Irecv loop and its chunk transposes, FFT_R2C.cu:48-66 / FFT_C2R.cu:48-66):
+ * the copies between the rank's field and its exchange buffer, and the sends
+ * and receives to each peer, in the order the slab plans issue them.  Host
+ * only (no device needed).  Each op is 10 int64: kind (0 local 2D copy,
+ * 1 send, 2 receive), peer, src buffer (0 field, 1 exchange buffer),
+ * src offset, src pitch, dst buffer, dst offset, dst pitch, width, rows
+ * (bytes).  fused != 0: the plans' Pass A writes / reads the exchange layout
+ * itself, so the local copies are left out.  Returns the number of ops, or
+ * minus the number needed when `cap` is too small. */
+int gpufft_dist_schedule(int64_t nx, int64_t ny, int64_t nz, int dtype, int procs, int rank, int forward, int fused,
+                         int64_t *ops, int cap);
 int gpufft_dgroup_exec(gpufft_dplan *plans, void **data, int procs, int forward, void *stream);
 
 /* --------------------------------------------------------------------------
