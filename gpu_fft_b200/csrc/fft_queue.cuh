@@ -31,7 +31,8 @@
 // items in list order from an atomic counter.  A second-phase item waits
 // (acquire load of the plane's completion count, bounded by a time limit,
 // then an error flag) until its plane's first phase is complete; first-
-// phase items publish with a release add after their stores.
+// phase items are published with a release add by the copy warp once their
+// buffer is released (after the consumers' stores).
 //
 // CTA roles: NT/32 consumer warps transform items; one producer warp (lane
 // 0) claims the next item, waits for its plane when needed and issues its
@@ -41,10 +42,11 @@
 //
 // Deadlock freedom: a CTA waits for a plane only in its producer, while its
 // consumers finish every item the CTA claimed earlier (they never wait on
-// anything but copies already issued).  Items are claimed in list order, so
-// the lowest-numbered unfinished item always belongs to a CTA that can
-// finish it: its dependencies have lower numbers and are finished.  This
-// holds however many CTAs are resident.
+// anything but copies already issued) and the producer keeps publishing them
+// during the wait.  Items are claimed in list order, so the lowest-numbered
+// unpublished item always belongs to a CTA that can finish and publish it:
+// its dependencies have lower numbers and are published.  This holds however
+// many CTAs are resident.
 //
 // Counters (plan-owned, int): [0] next item, [1] CTAs finished, [2] error
 // flag, [3] spare, [4 + x] items finished of plane x.  The last CTA to finish
@@ -257,7 +259,25 @@ __global__ void __launch_bounds__(NT + 32, 1)
         // ------------------------------ producer ------------------------------
         if (lane == 0) {
             bool err = false;
-            for (int k = 0;; ++k) {
+            // A first-phase item is published here, once the consumers have
+            // released its buffer: their stores precede their arrival on the
+            // empty barrier (block barrier, then arrive), which precedes this
+            // release at GPU scope.  The release waits for those stores to
+            // reach L2 -- on this otherwise idle warp, not on a consumer.
+            // Items are published in claim order; `pub` is the next one.  The
+            // dependency wait below keeps publishing the CTA's own finished
+            // items, so it never waits on an item of its own CTA.
+            int pub = 0;
+            auto publish = [&](int j) {
+                const int code = info[j % NBUF];
+                if (code >= 0 && ((code >> 15) & 1) == first_type) red_release_add(&ctr[4 + (code >> 16)], 1);
+            };
+            // publish items < upto that are finished, without waiting
+            auto try_publish = [&](int upto) {
+                while (pub < upto && mbar_try_wait(&empty[pub % NBUF], (uint32_t)((pub / NBUF) & 1))) publish(pub++);
+            };
+            int k = 0;
+            for (;; ++k) {
                 const int s = k % NBUF;
                 const uint32_t ph = (uint32_t)((k / NBUF) & 1);
                 if (!mbar_wait(&empty[s], ph ^ 1u, P.wait_ns)) {
@@ -266,11 +286,21 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     mbar_arrive(&full[s]);  // consumers may be waiting for this slot
                     break;
                 }
+                // items up to k - NBUF are finished (in order): publish them
+                // before slot s is reused
+                while (pub <= k - NBUF) publish(pub++);
                 const int g = atomicAdd(&ctr[0], 1);
                 const int it = g < P.nitems ? P.items[g] : -1;
                 info[s] = it;
                 if (it < 0) {
                     mbar_arrive(&full[s]);
+                    // publish the items still in the ring as they finish
+                    while (pub < k && !err) {
+                        if (!mbar_wait(&empty[pub % NBUF], (uint32_t)((pub / NBUF) & 1), P.wait_ns))
+                            err = true;
+                        else
+                            publish(pub++);
+                    }
                     break;
                 }
                 const int plane = it >> 16, type = (it >> 15) & 1, sub = it & 0x7fff;
@@ -279,6 +309,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     if (ld_acquire(cnt) < P.need) {
                         const unsigned long long t0 = globaltimer();
                         while (ld_acquire(cnt) < P.need) {
+                            try_publish(k);
                             __nanosleep(200);
                             // once any CTA has given up, the others stop waiting too
                             if ((long long)(globaltimer() - t0) > P.wait_ns || ld_acquire(&ctr[2]) != 0) {
@@ -436,10 +467,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 }
             }
             group_sync<NT>();  // stores issued, buffer reads done
-            if (tid == 0) {
-                if (type == first_type) red_release_add(&ctr[4 + plane], 1);
-                mbar_arrive(&empty[s]);
-            }
+            if (tid == 0) mbar_arrive(&empty[s]);  // the copy warp publishes the item
         }
     }
     __syncthreads();

@@ -223,9 +223,10 @@ static int max_clusters(const void *kernel, int K, int nx, size_t smem, int nt, 
 // then the table of 3-smooth lengths); candidate indices refer to it.
 static const std::vector<fast::VariantA> &variants_a(int dtype) {
     static const std::vector<fast::VariantA> f32 = [] {
-        std::vector<fast::VariantA> v(fast::kVariantsA_f32, fast::kVariantsA_f32 + fast::kNumVariantsA_f32);
+        // the queue form first: the default where it exists (512^2 planes)
+        std::vector<fast::VariantA> v(fast::kVariantsA_f32q, fast::kVariantsA_f32q + fast::kNumVariantsA_f32q);
+        v.insert(v.end(), fast::kVariantsA_f32, fast::kVariantsA_f32 + fast::kNumVariantsA_f32);
         v.insert(v.end(), fast::kVariantsA_f32s, fast::kVariantsA_f32s + fast::kNumVariantsA_f32s);
-        v.insert(v.end(), fast::kVariantsA_f32q, fast::kVariantsA_f32q + fast::kNumVariantsA_f32q);
         return v;
     }();
     static const std::vector<fast::VariantA> f64(fast::kVariantsA_f64, fast::kVariantsA_f64 + fast::kNumVariantsA_f64);
@@ -234,9 +235,10 @@ static const std::vector<fast::VariantA> &variants_a(int dtype) {
 
 static const std::vector<fast::VariantB> &variants_b(int dtype) {
     static const std::vector<fast::VariantB> f32 = [] {
-        std::vector<fast::VariantB> v(fast::kVariantsB_f32, fast::kVariantsB_f32 + fast::kNumVariantsB_f32);
+        // the tensor-copy form first: the default where it exists
+        std::vector<fast::VariantB> v(fast::kVariantsB_f32q, fast::kVariantsB_f32q + fast::kNumVariantsB_f32q);
+        v.insert(v.end(), fast::kVariantsB_f32, fast::kVariantsB_f32 + fast::kNumVariantsB_f32);
         v.insert(v.end(), fast::kVariantsB_f32s, fast::kVariantsB_f32s + fast::kNumVariantsB_f32s);
-        v.insert(v.end(), fast::kVariantsB_f32q, fast::kVariantsB_f32q + fast::kNumVariantsB_f32q);
         return v;
     }();
     static const std::vector<fast::VariantB> f64(fast::kVariantsB_f64, fast::kVariantsB_f64 + fast::kNumVariantsB_f64);

@@ -434,11 +434,22 @@ def test_pass_a_cluster_size_does_not_change_results(cuda, tmp_path, k):
     ref = f.clone()
     base = g.Plan(n, n, n, "float")
     base.r2c(ref)
+    # the cluster form's first candidate (the queue form comes first by default)
+    ca = None
+    for c in range(16):
+        os.environ["GPUFFT_VARIANT_A"] = str(c)
+        try:
+            if "fastA{kind=0 " in g.Plan(n, n, n, "float").describe():
+                ca = c
+                break
+        finally:
+            del os.environ["GPUFFT_VARIANT_A"]
+    assert ca is not None
     path = tmp_path / "w.txt"
     g.wisdom_save(str(path))
     dev = torch.cuda.get_device_name(0).replace(" ", "_")
     major, minor = torch.cuda.get_device_capability(0)
-    path.write_text(f"{dev}_sm{major * 10 + minor} 0 {n} {n} {n} 0 0 {k}\n")
+    path.write_text(f"{dev}_sm{major * 10 + minor} 0 {n} {n} {n} {ca} 0 {k}\n")
     g.wisdom_load(str(path))
     p = g.Plan(n, n, n, "float")
     assert (f"K={k} " if k > 0 else "split=1}") in p.describe(), p.describe()
