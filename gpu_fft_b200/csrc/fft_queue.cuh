@@ -69,8 +69,8 @@ using fast::ToSmem;
 struct PassAQParams {
     void *data;
     const void *unp;    // exp(-2 pi i k / Nz), k < M (the full unpack table)
-    const void *stz;    // per-stage tables of the z and y FFTs (fft_fast.cuh stage_offset)
-    const void *sty;
+    const void *rtw;    // row FFT step-1 twiddles: exp(-2 pi i a f / M) at (f - 1) * 16 + a, f < M / 16
+    const void *sty;    // per-stage table of the y FFT (fft_fast.cuh stage_offset)
     const int *items;   // work list: (plane << 16) | (type << 15) | sub
     int nitems;
     int *ctr;           // counters (header)
@@ -175,6 +175,7 @@ struct QShape {
     static constexpr int O_OFF = rup(E_BYTES);
     static constexpr int X_OFF = O_OFF + rup(O_BYTES);
     static constexpr int BUF = rup(mx(mx(ROW_BYTES, TILE_BYTES), X_OFF + X_BYTES));
+    static constexpr int R2 = M / 16;                // row FFT: M = 16 x R2
     static constexpr int TAB = rup((M + M + NY) * (int)sizeof(V));
     // tables, buffers, mbarriers, slot words, and slack for 128-byte alignment
     static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + 2 * NBUF * 8 + NBUF * 4 + 128; }
@@ -182,37 +183,35 @@ struct QShape {
     static_assert(NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
     static_assert(NY % RI == 0 && NY % 2 == 0 && BH <= 256, "rows per item / box height");
     static_assert(M % WY == 0, "whole column tiles");
-    static_assert(M == 256, "the row FFT is 16 x 16");
+    static_assert(M % 16 == 0 && (R2 == 8 || R2 == 16), "the row FFT is 16 x 8 or 16 x 16");
     static_assert(NT % 32 == 0 && NT == 16 * RI, "two rows per consumer warp");
     static_assert(WY % 2 == 0, "16-byte box rows");
 };
 
 // ---------------------------------------------------------------------------
-// one warp, two z-rows of M = 256 complex (16 lanes per row), in place in
-// the natural row layout.  Step 1: lane a transforms x[a + 16 n] over n and
-// twiddles by w_256^(a f); its outputs go to slot 16 f + (a ^ f) (an XOR
+// one warp, two z-rows of M = 16 R2 complex (16 lanes per row), in place in
+// the natural row layout.  Step 1: lane a transforms x[a + 16 n] over n < R2
+// and twiddles by w_M^(a f); its outputs go to slot 16 f + (a ^ f) (an XOR
 // swizzle: the writes of step 1 and the reads of step 2 are both
-// conflict-free).  Step 2: lane b transforms those of frequency b over a,
-// giving X[b + 16 j] in registers.  The per-stage table (stage 1 of the
-// 16 x 16 factorisation) holds w_256^(j k) at 15 + (j - 1) 16 + k, and the
-// twiddle is symmetric in (j, k): lane a reads entry (f, a), contiguous
-// across lanes.
+// conflict-free).  Step 2: lane b < R2 transforms those of frequency b over
+// a, giving X[b + R2 j], j < 16, in registers.  The twiddle table holds
+// w_M^(a f) at (f - 1) 16 + a: lanes read consecutive entries.
 // ---------------------------------------------------------------------------
-template <bool FWD, typename V>
-__device__ __forceinline__ void row256_step1(V (&x)[16], V *row, const V *stz, int a) {
-    Dft<16, FWD, V>::run(x);
+template <bool FWD, int R2, typename V>
+__device__ __forceinline__ void row_step1(V (&x)[R2], V *row, const V *rtw, int a) {
+    Dft<R2, FWD, V>::run(x);
 #pragma unroll
-    for (int f = 1; f < 16; ++f) x[f] = c_tw<FWD>(x[f], stz[15 + (f - 1) * 16 + a]);
+    for (int f = 1; f < R2; ++f) x[f] = c_tw<FWD>(x[f], rtw[(f - 1) * 16 + a]);
     __syncwarp();  // every lane has read its inputs before the row is overwritten
 #pragma unroll
-    for (int f = 0; f < 16; ++f) row[16 * f + (a ^ f)] = x[f];
+    for (int f = 0; f < R2; ++f) row[16 * f + (a ^ f)] = x[f];
     __syncwarp();
 }
 template <bool FWD, typename V>
-__device__ __forceinline__ void row256_step2(V (&x)[16], const V *row, int b) {
+__device__ __forceinline__ void row_step2(V (&y)[16], const V *row, int b) {
 #pragma unroll
-    for (int a = 0; a < 16; ++a) x[a] = row[16 * b + (a ^ b)];
-    Dft<16, FWD, V>::run(x);
+    for (int a = 0; a < 16; ++a) y[a] = row[16 * b + (a ^ b)];
+    Dft<16, FWD, V>::run(y);
 }
 
 // ---------------------------------------------------------------------------
@@ -226,20 +225,20 @@ __global__ void __launch_bounds__(NT + 32, 1)
     using V = cx_t<T>;
     using ColFFT = TileFFT<T, NY, S::WY, NT, FWD, COLS, VY, GROUP>;
     using ColL = typename ColFFT::L;
-    constexpr int NH = S::NH, WY = S::WY, RI = S::RI, BH = S::BH;
+    constexpr int NH = S::NH, WY = S::WY, RI = S::RI, BH = S::BH, R2 = S::R2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // copy destinations are 128-byte aligned (smem_bytes() reserves the slack)
     unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     V *unp = reinterpret_cast<V *>(smem);
-    V *stz = unp + M;
-    V *sty = stz + M;
+    V *rtw = unp + M;
+    V *sty = rtw + M;
     unsigned char *bufs = smem + S::TAB;
     uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF);
     uint64_t *empty = full + NBUF;
     int *info = reinterpret_cast<int *>(empty + NBUF);
 
     for (int q = threadIdx.x; q < M; q += blockDim.x) unp[q] = reinterpret_cast<const V *>(P.unp)[q];
-    for (int q = threadIdx.x; q < M - 1; q += blockDim.x) stz[q] = reinterpret_cast<const V *>(P.stz)[q];
+    for (int q = threadIdx.x; q < 16 * (R2 - 1); q += blockDim.x) rtw[q] = reinterpret_cast<const V *>(P.rtw)[q];
     for (int q = threadIdx.x; q < NY - 1; q += blockDim.x) sty[q] = reinterpret_cast<const V *>(P.sty)[q];
     if (threadIdx.x == 0) {
         for (int s = 0; s < NBUF; ++s) {
@@ -362,23 +361,32 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 const int r = 2 * warp + h;
                 V *row = reinterpret_cast<V *>(b) + r * NH;
                 V *grow = gplane + ((long long)sub * RI + r) * NH;
-                V x[16];
+                V x[R2];
                 if constexpr (FWD) {
 #pragma unroll
-                    for (int n = 0; n < 16; ++n) x[n] = row[a + 16 * n];
-                    row256_step1<true>(x, row, stz, a);
-                    row256_step2<true>(x, row, a);
-                    __syncwarp();  // step 2's reads are done before X is stored
+                    for (int n = 0; n < R2; ++n) x[n] = row[a + 16 * n];
+                    row_step1<true, R2>(x, row, rtw, a);
+                    {
+                        V y[16];
+                        if (R2 == 16 || a < R2) row_step2<true>(y, row, a);
+                        __syncwarp();  // step 2's reads are done before X is stored
+                        if (R2 == 16 || a < R2) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) row[a + 16 * j] = x[j];
+                            for (int j = 0; j < 16; ++j) row[a + R2 * j] = y[j];
+                        }
+                        if constexpr (R2 == 16) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) x[j] = y[j];  // X[a + 16 j] stays in registers
+                        }
+                    }
                     __syncwarp();
                     // unpack: X[k] = E + O, E = (Z[k] + conj Z[M-k]) / 2,
                     // O = -i w^k (Z[k] - conj Z[M-k]) / 2; bins 0 and M packed in slot 0
                     const T hf = (T)0.5;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
+                    for (int j = 0; j < R2; ++j) {
                         const int kk = a + 16 * j;
-                        const V za = x[j];
+                        const V za = R2 == 16 ? x[j] : row[kk];
                         const V zb = c_conj(row[(M - kk) & (M - 1)]);
                         const V e = c_scale(c_add(za, zb), hf);
                         const V d = c_scale(c_sub(za, zb), hf);
@@ -395,7 +403,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     // pack: Z[k] = S + Pk, S = X[k] + conj X[M-k], Pk = i conj(w^k) (X[k] - conj X[M-k]);
                     // slot 0 holds (Re X0, Re XM)
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
+                    for (int j = 0; j < R2; ++j) {
                         const int kk = a + 16 * j;
                         V xa = row[kk], xb = row[(M - kk) & (M - 1)];
                         if (kk == 0) {
@@ -407,10 +415,13 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         const V pk = c_rot<false>(c_mulc(c_sub(xa, cm), unp[kk]));
                         x[j] = c_add(sv, pk);
                     }
-                    row256_step1<false>(x, row, stz, a);
-                    row256_step2<false>(x, row, a);
+                    row_step1<false, R2>(x, row, rtw, a);
+                    if (R2 == 16 || a < R2) {
+                        V y[16];
+                        row_step2<false>(y, row, a);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) st_g(grow + a + 16 * j, x[j]);
+                        for (int j = 0; j < 16; ++j) st_g(grow + a + R2 * j, y[j]);
+                    }
                     if (a == 0) st_g(grow + M, V{(T)0, (T)0});  // padding cells of the real row
                 }
             } else {
@@ -496,6 +507,9 @@ __global__ void __launch_bounds__(NT + 32, 1)
 // tiles b, b + grid, ...; NBUF tiles are in flight, and thread 0 issues the
 // copies of tile k + NBUF as soon as the barrier after tile k's FFT has freed
 // its buffer (no copy-issuing warp, so every warp's registers go to the FFT).
+// NBUF = 1 (tiles too large for two buffers: Nx = 1024) refills the one
+// buffer as soon as the last FFT stage has read it (TileFFT::run's hook),
+// so the next tile streams in while that stage computes and stores.
 // ---------------------------------------------------------------------------
 template <typename T, int NX, int NT, int NBUF>
 struct BShape {
@@ -563,12 +577,23 @@ __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const _
             }
         };
         FromSmem fs;
-        FFT::run(fs, dst, tile, tw);
-        __syncthreads();  // every read of the tile is done: refill its buffer
         const long long tn = t + (long long)NBUF * gridDim.x;
-        if (threadIdx.x == 0 && tn < P.ntiles) {
-            fence_proxy_async_shared();
-            issue(tn, s);
+        if constexpr (NBUF == 1) {
+            static_assert(FFT::NS >= 2, "the first stage must read the tile from shared memory");
+            auto refill = [&]() {  // (called by every thread after the last stage's reads and a barrier)
+                if (threadIdx.x == 0 && tn < P.ntiles) {
+                    fence_proxy_async_shared();
+                    issue(tn, s);
+                }
+            };
+            FFT::run(fs, dst, tile, tw, refill);
+        } else {
+            FFT::run(fs, dst, tile, tw);
+            __syncthreads();  // every read of the tile is done: refill its buffer
+            if (threadIdx.x == 0 && tn < P.ntiles) {
+                fence_proxy_async_shared();
+                issue(tn, s);
+            }
         }
     }
 }

@@ -264,6 +264,7 @@ static void free_queue(Plan &P) {
     P.q_dev = nullptr;
     P.q_items_f = P.q_items_i = nullptr;
     P.q_unp = nullptr;
+    P.q_rtw = nullptr;
 }
 
 // Work list of one direction: block b holds the first-phase items of plane b
@@ -295,18 +296,32 @@ static int setup_queue(Plan &P) {
     const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
     const int ri = (P.fa->nt - 32) / 16, wy = P.fa->wy;  // two rows per consumer warp
     const int nri = ny / ri, nci = m / wy;
-    int depth = P.kfix > 0 ? P.kfix : 8;
+    // default depth: about 768 items between a plane's two phases (at 512^3,
+    // 32 items per plane, depths 16-32 measured best; at 512 x 128 planes,
+    // 24 items per plane, 32)
+    int depth = P.kfix > 0 ? P.kfix : std::max(8, std::min(64, 768 / std::max(1, nri + nci)));
     if (const char *ev = std::getenv("GPUFFT_QUEUE_DEPTH")) depth = std::atoi(ev);
     depth = std::max(1, std::min(nx, depth));
     const std::vector<int> fwd = queue_items(nx, nri, nci, q::ROW_ITEM, depth);
     const std::vector<int> inv = queue_items(nx, nci, nri, q::COL_ITEM, depth);
-    std::vector<float> unp(2 * (size_t)m);
+    // unpack roots exp(-2 pi i k / Nz), k < M, then the row FFT's step-1
+    // twiddles exp(-2 pi i a f / M) at (f - 1) * 16 + a (M = 16 * R2): FP64-class
+    // host values rounded once
+    const int r2 = m / 16;
+    std::vector<float> unp(2 * (size_t)m + 2 * 16 * (size_t)std::max(r2 - 1, 0));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int k = 0; k < m; ++k) {
         const long double ang = two_pi * (long double)k / (long double)(2 * m);
         unp[2 * k] = (float)cosl(ang);
         unp[2 * k + 1] = (float)(-sinl(ang));
     }
+    for (int f = 1; f < r2; ++f)
+        for (int a = 0; a < 16; ++a) {
+            const size_t at = 2 * (size_t)m + 2 * ((size_t)(f - 1) * 16 + a);
+            const long double ang = two_pi * (long double)((a * f) % m) / (long double)m;
+            unp[at] = (float)cosl(ang);
+            unp[at + 1] = (float)(-sinl(ang));
+        }
     const size_t cbytes = ((size_t)(4 + nx) * sizeof(int) + 255) / 256 * 256;
     const size_t lbytes = (fwd.size() * sizeof(int) + 255) / 256 * 256;
     const size_t ubytes = unp.size() * sizeof(float);
@@ -330,6 +345,7 @@ static int setup_queue(Plan &P) {
     P.q_items_f = reinterpret_cast<const int *>(b + cbytes);
     P.q_items_i = reinterpret_cast<const int *>(b + cbytes + lbytes);
     P.q_unp = b + cbytes + 2 * lbytes;
+    P.q_rtw = b + cbytes + 2 * lbytes + 2 * (size_t)m * sizeof(float);
     return GPUFFT_SUCCESS;
 }
 
@@ -414,7 +430,7 @@ static int setup_fast(Plan &P, int idx_a, int idx_b) {
         // planes in flight with shorter barriers (512^3 FP32 takes 4 over 8),
         // 16-CTA clusters (non-portable) put fewer in flight when planes are
         // large (1024^2)
-        if (P.kfix > 0 && P.fa->kind == 0) {
+        if (P.kfix > 0 && P.kfix <= 16 && P.fa->kind == 0) {  // (a queue form's kfix is its depth)
             K = std::min(P.kfix, std::max(1, ny));
             if (K > 8) {
                 for (const void *k : {P.fa->kfwd, P.fa->kinv, P.fa->kfwd_x, P.fa->kinv_x})
@@ -628,9 +644,9 @@ int plan_autotune(Plan *P, void *scratch, void *stream) {
                         if (k >= 2) ks[nk++] = k;
                     ks[nk++] = -1;
                 } else if (P->fa && P->fa->kind == 2) {
-                    // the queue form: planes between a plane's two phases (default 8)
-                    ks[nk++] = 4;
+                    // the queue form: planes between a plane's two phases
                     ks[nk++] = 16;
+                    ks[nk++] = 32;
                 }
             }
             for (int ki = 0; ki < nk; ++ki) {
@@ -876,7 +892,7 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
         q::PassAQParams qp{};
         qp.data = data;
         qp.unp = P.q_unp;
-        qp.stz = P.pa.stz;
+        qp.rtw = P.q_rtw;
         qp.sty = P.pa.sty;
         qp.items = fwd ? P.q_items_f : P.q_items_i;
         qp.nitems = P.q_nitems;

@@ -40,6 +40,7 @@ struct Plan {
     int q_need = 0;      // first-phase items per plane (forward)
     const int *q_items_f = nullptr, *q_items_i = nullptr;
     const void *q_unp = nullptr;
+    const void *q_rtw = nullptr;  // the row FFT's step-1 twiddles
 };
 
 int set_error(int code, const char *fmt, ...);

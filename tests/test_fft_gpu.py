@@ -432,9 +432,8 @@ def test_pass_a_cluster_size_does_not_change_results(cuda, tmp_path, k):
     f = torch.zeros((n, n, n + 2), device="cuda")
     f[:, :, :n] = torch.randn((n, n, n), generator=gen, device="cuda")
     ref = f.clone()
-    base = g.Plan(n, n, n, "float")
-    base.r2c(ref)
-    # the cluster form's first candidate (the queue form comes first by default)
+    # the cluster form's first candidate (the queue form comes first by
+    # default), at the cluster size chosen from the L2 size
     ca = None
     for c in range(16):
         os.environ["GPUFFT_VARIANT_A"] = str(c)
@@ -445,6 +444,12 @@ def test_pass_a_cluster_size_does_not_change_results(cuda, tmp_path, k):
         finally:
             del os.environ["GPUFFT_VARIANT_A"]
     assert ca is not None
+    os.environ["GPUFFT_VARIANT_A"] = str(ca)
+    try:
+        base = g.Plan(n, n, n, "float")
+    finally:
+        del os.environ["GPUFFT_VARIANT_A"]
+    base.r2c(ref)
     path = tmp_path / "w.txt"
     g.wisdom_save(str(path))
     dev = torch.cuda.get_device_name(0).replace(" ", "_")
