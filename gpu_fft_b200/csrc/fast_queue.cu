@@ -24,6 +24,9 @@ const VariantA kVariantsA_f32q[] = {
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),
+    // 360 x 240 planes (384 x 360 x 480): the row FFT is 16 x 15 (prime-factor
+    // radix 15), 24-row items on 12 consumer warps, 4-deep ring of 52 KB buffers
+    QA_ENTRY(float, 0, 360, 240, 384, 0, 4, 16),
 };
 const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[0]);
 

@@ -183,7 +183,7 @@ struct QShape {
     static_assert(NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
     static_assert(NY % RI == 0 && NY % 2 == 0 && BH <= 256, "rows per item / box height");
     static_assert(M % WY == 0, "whole column tiles");
-    static_assert(M % 16 == 0 && (R2 == 8 || R2 == 16), "the row FFT is 16 x 8 or 16 x 16");
+    static_assert(M % 16 == 0 && (R2 == 8 || R2 == 15 || R2 == 16), "the row FFT is 16 x 8, 16 x 15 or 16 x 16");
     static_assert(NT % 32 == 0 && NT == 16 * RI, "two rows per consumer warp");
     static_assert(WY % 2 == 0, "16-byte box rows");
 };
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     for (int j = 0; j < R2; ++j) {
                         const int kk = a + 16 * j;
                         const V za = R2 == 16 ? x[j] : row[kk];
-                        const V zb = c_conj(row[(M - kk) & (M - 1)]);
+                        const V zb = c_conj(row[(kk == 0 ? 0 : M - kk)]);
                         const V e = c_scale(c_add(za, zb), hf);
                         const V d = c_scale(c_sub(za, zb), hf);
                         const V o = c_rot<true>(c_mul(d, unp[kk]));
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
                         const int kk = a + 16 * j;
-                        V xa = row[kk], xb = row[(M - kk) & (M - 1)];
+                        V xa = row[kk], xb = row[(kk == 0 ? 0 : M - kk)];
                         if (kk == 0) {
                             xb = V{xa.y, (T)0};
                             xa = V{xa.x, (T)0};

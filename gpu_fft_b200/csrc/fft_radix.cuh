@@ -364,6 +364,31 @@ template <int R, bool FWD, typename V> struct DftOdd {
     }
 };
 template <bool FWD, typename V> struct Dft<3, FWD, V> : DftOdd<3, FWD, V> {};
+// radix 15 = 3 x 5 by the prime-factor (Good-Thomas) map, no twiddles:
+// input n = (5 n1 + 3 n2) mod 15, output k = (10 k1 + 6 k2) mod 15; DFT3 over
+// n1 for each n2, then DFT5 over n2 for each k1
+template <bool FWD, typename V> struct Dft<15, FWD, V> {
+    static __device__ __forceinline__ void run(V *x) {
+        V y[5][3];
+#pragma unroll
+        for (int n2 = 0; n2 < 5; ++n2) {
+            V a = x[(3 * n2) % 15], b = x[(5 + 3 * n2) % 15], c = x[(10 + 3 * n2) % 15];
+            dft3<FWD>(a, b, c);
+            y[n2][0] = a;
+            y[n2][1] = b;
+            y[n2][2] = c;
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            V b[5];
+#pragma unroll
+            for (int n2 = 0; n2 < 5; ++n2) b[n2] = y[n2][k1];
+            DftOdd<5, FWD, V>::run(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 5; ++k2) x[(10 * k1 + 6 * k2) % 15] = b[k2];
+        }
+    }
+};
 template <bool FWD, typename V> struct Dft<5, FWD, V> : DftOdd<5, FWD, V> {};
 template <bool FWD, typename V> struct Dft<7, FWD, V> : DftOdd<7, FWD, V> {};
 template <bool FWD, typename V> struct Dft<11, FWD, V> : DftOdd<11, FWD, V> {};
