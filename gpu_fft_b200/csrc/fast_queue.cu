@@ -52,5 +52,19 @@ const VariantB kVariantsB_f32q[] = {
 };
 const int kNumVariantsB_f32q = sizeof(kVariantsB_f32q) / sizeof(kVariantsB_f32q[0]);
 
+// FP64: 16-row items on 8 consumer warps (the radix-16 row butterflies need
+// 64 registers of data), 8-column (128-byte) items, a 2-deep ring (three
+// 72 KB buffers and the 16 KB of tables do not fit)
+const VariantA kVariantsA_f64q[] = {
+    QA_ENTRY(double, 1, 512, 256, 256, 0, 2, 8),
+};
+const int kNumVariantsA_f64q = sizeof(kVariantsA_f64q) / sizeof(kVariantsA_f64q[0]);
+
+const VariantB kVariantsB_f64q[] = {
+    TB_ENTRY(double, 1, 512, 256, 0, 2),
+    TB_ENTRY(double, 1, 512, 512, 0, 2),
+};
+const int kNumVariantsB_f64q = sizeof(kVariantsB_f64q) / sizeof(kVariantsB_f64q[0]);
+
 }  // namespace fast
 }  // namespace gpufft

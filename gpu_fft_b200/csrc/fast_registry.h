@@ -51,6 +51,10 @@ extern const VariantA kVariantsA_f32q[];  // queue-scheduled Pass A (fast_queue.
 extern const int kNumVariantsA_f32q;
 extern const VariantB kVariantsB_f32q[];  // tensor-copy Pass B (fast_queue.cu)
 extern const int kNumVariantsB_f32q;
+extern const VariantA kVariantsA_f64q[];  // FP64 queue form and tensor-copy x pass (fast_queue.cu)
+extern const int kNumVariantsA_f64q;
+extern const VariantB kVariantsB_f64q[];
+extern const int kNumVariantsB_f64q;
 extern const VariantA kVariantsA_f64[];
 extern const int kNumVariantsA_f64;
 extern const VariantB kVariantsB_f64[];

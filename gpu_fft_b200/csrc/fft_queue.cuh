@@ -156,18 +156,25 @@ __device__ __forceinline__ void group_sync() {
 // ---------------------------------------------------------------------------
 // shape of one instantiation
 // ---------------------------------------------------------------------------
+// FP32 (PAIR): the row-pair view above, boxes E and O of NY/2 lines each.
+// FP64: rows are 16-byte aligned on their own; the view is [rows][2 Nh]
+// 8-byte elements and box E is WY columns of every row (NBX boxes of BHT
+// rows), box X the one column M of every row.
 template <typename T, int NY, int M, int NT, int NBUF, int WY_>
 struct QShape {
     using V = cx_t<T>;
+    static constexpr bool PAIR = sizeof(V) == 8;
     static constexpr int NH = M + 1;
     static constexpr int WY = WY_;                   // columns per column item
     static constexpr int RI = NT / 16;               // rows per row item (two per consumer warp)
-    static constexpr int BH = NY / 2;                // row pairs per box
+    static constexpr int BH = NY / 2;                // row pairs per box (PAIR)
+    static constexpr int BHT = NY > 256 ? 256 : NY;  // rows per box (FP64)
+    static constexpr int NBX = NY / BHT;
     static constexpr int NRI = NY / RI;
     static constexpr int NCI = M / WY;
-    static constexpr int E_BYTES = WY * BH * (int)sizeof(V);
-    static constexpr int O_BYTES = (WY + 2) * BH * (int)sizeof(V);
-    static constexpr int X_BYTES = 2 * BH * (int)sizeof(V);
+    static constexpr int E_BYTES = PAIR ? WY * BH * (int)sizeof(V) : WY * NY * (int)sizeof(V);
+    static constexpr int O_BYTES = PAIR ? (WY + 2) * BH * (int)sizeof(V) : 0;
+    static constexpr int X_BYTES = PAIR ? 2 * BH * (int)sizeof(V) : NY * (int)sizeof(V);
     static constexpr int ROW_BYTES = RI * NH * (int)sizeof(V);
     static constexpr int TILE_BYTES = NY * WY * (int)sizeof(V);
     static constexpr int rup(int v) { return (v + 127) / 128 * 128; }
@@ -179,13 +186,14 @@ struct QShape {
     static constexpr int TAB = rup((M + M + NY) * (int)sizeof(V));
     // tables, buffers, mbarriers, slot words, and slack for 128-byte alignment
     static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + 2 * NBUF * 8 + NBUF * 4 + 128; }
-    static_assert(sizeof(V) == 8, "row-pair view: FP32 complex");
-    static_assert(NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
-    static_assert(NY % RI == 0 && NY % 2 == 0 && BH <= 256, "rows per item / box height");
+    static_assert(!PAIR || NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
+    static_assert(!PAIR || BH <= 256, "box height");
+    static_assert(PAIR || NY % BHT == 0, "whole boxes");
+    static_assert(NY % RI == 0 && NY % 2 == 0, "rows per item");
     static_assert(M % WY == 0, "whole column tiles");
     static_assert(M % 16 == 0 && (R2 == 8 || R2 == 15 || R2 == 16), "the row FFT is 16 x 8, 16 x 15 or 16 x 16");
     static_assert(NT % 32 == 0 && NT == 16 * RI, "two rows per consumer warp");
-    static_assert(WY % 2 == 0, "16-byte box rows");
+    static_assert(!PAIR || WY % 2 == 0, "16-byte box rows");
 };
 
 // ---------------------------------------------------------------------------
@@ -327,12 +335,24 @@ __global__ void __launch_bounds__(NT + 32, 1)
                               &full[s]);
                 } else {
                     const int c0 = sub * WY;
-                    const int y = plane * BH;
                     const bool xtra = !FWD && sub == 0;
                     mbar_arrive_expect_tx(&full[s], (uint32_t)(S::E_BYTES + S::O_BYTES + (xtra ? S::X_BYTES : 0)));
-                    tensor_load_2d(b, &tm_e, c0, y, &full[s]);
-                    tensor_load_2d(b + S::O_OFF, &tm_o, NH - 1 + c0, y, &full[s]);
-                    if (xtra) tensor_load_2d(b + S::X_OFF, &tm_x, 2 * NH - 2, y, &full[s]);
+                    if constexpr (S::PAIR) {
+                        const int y = plane * BH;
+                        tensor_load_2d(b, &tm_e, c0, y, &full[s]);
+                        tensor_load_2d(b + S::O_OFF, &tm_o, NH - 1 + c0, y, &full[s]);
+                        if (xtra) tensor_load_2d(b + S::X_OFF, &tm_x, 2 * NH - 2, y, &full[s]);
+                    } else {
+                        constexpr int EPC = (int)sizeof(V) / 8;  // 8-byte elements per complex
+#pragma unroll
+                        for (int q = 0; q < S::NBX; ++q) {
+                            const int y = plane * NY + q * S::BHT;
+                            tensor_load_2d(b + (size_t)q * S::BHT * WY * sizeof(V), &tm_e, EPC * c0, y, &full[s]);
+                            if (xtra)
+                                tensor_load_2d(b + S::X_OFF + (size_t)q * S::BHT * sizeof(V), &tm_x, EPC * M, y,
+                                               &full[s]);
+                        }
+                    }
                 }
             }
             if (err) atomicExch(&ctr[2], 1);
@@ -432,7 +452,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 const V *bx = reinterpret_cast<const V *>(b + S::X_OFF);
                 V *tile = reinterpret_cast<V *>(b);
                 auto at = [&](int n, int w) -> V {
-                    return (n & 1) ? bo[(n >> 1) * (WY + 2) + 1 + w] : be[(n >> 1) * WY + w];
+                    if constexpr (S::PAIR)
+                        return (n & 1) ? bo[(n >> 1) * (WY + 2) + 1 + w] : be[(n >> 1) * WY + w];
+                    else
+                        return be[n * WY + w];
                 };
                 auto dst = [&](int n, int w, V v) { st_g(gplane + (long long)n * NH + c0 + w, v); };
                 if constexpr (FWD) {
@@ -463,7 +486,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     // along y, packed as a' + i b' into column 0
                     const T hf = (T)0.5;
                     auto binm = [&](int n) -> V {
-                        return (n & 1) ? bx[(n >> 1) * 2 + 1] : bo[(n >> 1) * (WY + 2)];
+                        if constexpr (S::PAIR)
+                            return (n & 1) ? bx[(n >> 1) * 2 + 1] : bo[(n >> 1) * (WY + 2)];
+                        else
+                            return bx[n];
                     };
                     auto src = [&](int n, int w) -> V {
                         if (sub == 0 && w == 0) {
@@ -521,7 +547,7 @@ struct BShape {
     static constexpr int BUF = (TILE_BYTES + 127) / 128 * 128;
     static constexpr int TAB = ((NX * (int)sizeof(V)) + 127) / 128 * 128;
     static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + NBUF * 8 + 128; }
-    static_assert(sizeof(V) == 8, "FP32 complex");
+    static constexpr int EPC = (int)sizeof(V) / 8;   // 8-byte elements per complex
     static_assert(NX % BOXH == 0, "whole boxes");
 };
 
@@ -543,7 +569,7 @@ __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const _
         mbar_arrive_expect_tx(&full[s], (uint32_t)S::TILE_BYTES);
 #pragma unroll
         for (int bx = 0; bx < S::NBOX; ++bx)
-            tensor_load_2d(b + (size_t)bx * S::BOXH * W * sizeof(V), &tm, (int)(t * W), bx * S::BOXH, &full[s]);
+            tensor_load_2d(b + (size_t)bx * S::BOXH * W * sizeof(V), &tm, (int)(t * W * S::EPC), bx * S::BOXH, &full[s]);
     };
     if (threadIdx.x == 0) {
         for (int s = 0; s < NBUF; ++s) mbar_init(&full[s], 1);

@@ -229,7 +229,11 @@ static const std::vector<fast::VariantA> &variants_a(int dtype) {
         v.insert(v.end(), fast::kVariantsA_f32s, fast::kVariantsA_f32s + fast::kNumVariantsA_f32s);
         return v;
     }();
-    static const std::vector<fast::VariantA> f64(fast::kVariantsA_f64, fast::kVariantsA_f64 + fast::kNumVariantsA_f64);
+    static const std::vector<fast::VariantA> f64 = [] {
+        std::vector<fast::VariantA> v(fast::kVariantsA_f64q, fast::kVariantsA_f64q + fast::kNumVariantsA_f64q);
+        v.insert(v.end(), fast::kVariantsA_f64, fast::kVariantsA_f64 + fast::kNumVariantsA_f64);
+        return v;
+    }();
     return dtype == GPUFFT_FLOAT ? f32 : f64;
 }
 
@@ -241,7 +245,11 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
         v.insert(v.end(), fast::kVariantsB_f32s, fast::kVariantsB_f32s + fast::kNumVariantsB_f32s);
         return v;
     }();
-    static const std::vector<fast::VariantB> f64(fast::kVariantsB_f64, fast::kVariantsB_f64 + fast::kNumVariantsB_f64);
+    static const std::vector<fast::VariantB> f64 = [] {
+        std::vector<fast::VariantB> v(fast::kVariantsB_f64q, fast::kVariantsB_f64q + fast::kNumVariantsB_f64q);
+        v.insert(v.end(), fast::kVariantsB_f64, fast::kVariantsB_f64 + fast::kNumVariantsB_f64);
+        return v;
+    }();
     return dtype == GPUFFT_FLOAT ? f32 : f64;
 }
 
@@ -296,10 +304,10 @@ static int setup_queue(Plan &P) {
     const int nx = (int)P.nx, ny = (int)P.ny, m = (int)(P.nz / 2);
     const int ri = (P.fa->nt - 32) / 16, wy = P.fa->wy;  // two rows per consumer warp
     const int nri = ny / ri, nci = m / wy;
-    // default depth: about 768 items between a plane's two phases (at 512^3,
-    // 32 items per plane, depths 16-32 measured best; at 512 x 128 planes,
-    // 24 items per plane, 32)
-    int depth = P.kfix > 0 ? P.kfix : std::max(8, std::min(64, 768 / std::max(1, nri + nci)));
+    // default depth: about 1024 items between a plane's two phases (measured
+    // best: 16-32 planes of 32 items at 512^3, 32 of 24 items at 512 x 128
+    // planes, 32-48 of 30 items at 360 x 240 planes)
+    int depth = P.kfix > 0 ? P.kfix : std::max(8, std::min(64, 1024 / std::max(1, nri + nci)));
     if (const char *ev = std::getenv("GPUFFT_QUEUE_DEPTH")) depth = std::atoi(ev);
     depth = std::max(1, std::min(nx, depth));
     const std::vector<int> fwd = queue_items(nx, nri, nci, q::ROW_ITEM, depth);
@@ -308,23 +316,34 @@ static int setup_queue(Plan &P) {
     // twiddles exp(-2 pi i a f / M) at (f - 1) * 16 + a (M = 16 * R2): FP64-class
     // host values rounded once
     const int r2 = m / 16;
-    std::vector<float> unp(2 * (size_t)m + 2 * 16 * (size_t)std::max(r2 - 1, 0));
+    std::vector<double> unp(2 * (size_t)m + 2 * 16 * (size_t)std::max(r2 - 1, 0));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int k = 0; k < m; ++k) {
         const long double ang = two_pi * (long double)k / (long double)(2 * m);
-        unp[2 * k] = (float)cosl(ang);
-        unp[2 * k + 1] = (float)(-sinl(ang));
+        unp[2 * k] = (double)cosl(ang);
+        unp[2 * k + 1] = (double)(-sinl(ang));
     }
     for (int f = 1; f < r2; ++f)
         for (int a = 0; a < 16; ++a) {
             const size_t at = 2 * (size_t)m + 2 * ((size_t)(f - 1) * 16 + a);
             const long double ang = two_pi * (long double)((a * f) % m) / (long double)m;
-            unp[at] = (float)cosl(ang);
-            unp[at + 1] = (float)(-sinl(ang));
+            unp[at] = (double)cosl(ang);
+            unp[at + 1] = (double)(-sinl(ang));
         }
+    // rounded once to the plan's precision
+    const size_t tsz = P.dtype == GPUFFT_FLOAT ? sizeof(float) : sizeof(double);
+    std::vector<unsigned char> tab(unp.size() * tsz);
+    for (size_t i = 0; i < unp.size(); ++i) {
+        if (tsz == sizeof(float)) {
+            const float v = (float)unp[i];
+            std::memcpy(tab.data() + i * tsz, &v, tsz);
+        } else {
+            std::memcpy(tab.data() + i * tsz, &unp[i], tsz);
+        }
+    }
     const size_t cbytes = ((size_t)(4 + nx) * sizeof(int) + 255) / 256 * 256;
     const size_t lbytes = (fwd.size() * sizeof(int) + 255) / 256 * 256;
-    const size_t ubytes = unp.size() * sizeof(float);
+    const size_t ubytes = tab.size();
     cudaError_t e = cudaMalloc(&P.q_dev, cbytes + 2 * lbytes + ubytes);
     if (e != cudaSuccess) {
         P.q_dev = nullptr;
@@ -334,7 +353,7 @@ static int setup_queue(Plan &P) {
     e = cudaMemset(b, 0, cbytes);
     if (e == cudaSuccess) e = cudaMemcpy(b + cbytes, fwd.data(), fwd.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b + cbytes + lbytes, inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(b + cbytes + 2 * lbytes, unp.data(), ubytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b + cbytes + 2 * lbytes, tab.data(), ubytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         free_queue(P);
         return cuda_error(e, "upload Pass A queue state");
@@ -345,7 +364,7 @@ static int setup_queue(Plan &P) {
     P.q_items_f = reinterpret_cast<const int *>(b + cbytes);
     P.q_items_i = reinterpret_cast<const int *>(b + cbytes + lbytes);
     P.q_unp = b + cbytes + 2 * lbytes;
-    P.q_rtw = b + cbytes + 2 * lbytes + 2 * (size_t)m * sizeof(float);
+    P.q_rtw = b + cbytes + 2 * lbytes + 2 * (size_t)m * tsz;
     return GPUFFT_SUCCESS;
 }
 
@@ -364,18 +383,25 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// The row-pair view of an FP32 field with Nh odd: lines of 2*Nh 8-byte
-// elements (rows 2r and 2r+1), Nx*Ny/2 lines, line pitch 16*Nh bytes.
-static bool encode_pair_map(CUtensorMap *m, void *data, long long nh, long long lines, int box_w, int box_h) {
+// A 2D view of the field in 8-byte elements: `width` elements per line,
+// `lines` lines `pitch` bytes apart, boxes of box_w x box_h.
+static bool encode_view(CUtensorMap *m, void *data, long long width, long long lines, long long pitch, int box_w,
+                        int box_h) {
     const auto enc = tensor_map_encoder();
     if (!enc) return false;
-    const cuuint64_t dims[2] = {(cuuint64_t)(2 * nh), (cuuint64_t)lines};
-    const cuuint64_t strides[1] = {(cuuint64_t)(2 * nh * 8)};
+    const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)lines};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch};
     const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
     const cuuint32_t es[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, data, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The row-pair view of an FP32 field with Nh odd: lines of 2*Nh 8-byte
+// elements (rows 2r and 2r+1), Nx*Ny/2 lines, line pitch 16*Nh bytes.
+static bool encode_pair_map(CUtensorMap *m, void *data, long long nh, long long lines, int box_w, int box_h) {
+    return encode_view(m, data, 2 * nh, lines, 2 * nh * 8, box_w, box_h);
 }
 
 // Picks the specialised kernels for this plan's shape (first registry entry,
@@ -883,12 +909,24 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
     }
     if (P.fa && P.fa->kind == 2 && !xch && ((uintptr_t)data) % 16 == 0) {
         // queue-scheduled Pass A: the tensor maps carry this call's field address
-        const long long nh = P.nz / 2 + 1, lines = P.nx * P.ny / 2;
-        const int wy = P.fa->wy, bh = (int)(P.ny / 2);
+        const long long nh = P.nz / 2 + 1;
+        const int wy = P.fa->wy;
         CUtensorMap tm[3];
-        if (!encode_pair_map(&tm[0], data, nh, lines, wy, bh) || !encode_pair_map(&tm[1], data, nh, lines, wy + 2, bh) ||
-            !encode_pair_map(&tm[2], data, nh, lines, 2, bh))
-            return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass A field view");
+        bool ok;
+        if (P.dtype == GPUFFT_FLOAT) {
+            // row pairs: lines of 2 Nh complex, boxes of Ny/2 lines
+            const long long lines = P.nx * P.ny / 2;
+            const int bh = (int)(P.ny / 2);
+            ok = encode_pair_map(&tm[0], data, nh, lines, wy, bh) && encode_pair_map(&tm[1], data, nh, lines, wy + 2, bh) &&
+                 encode_pair_map(&tm[2], data, nh, lines, 2, bh);
+        } else {
+            // single rows: 2 Nh 8-byte elements per row (16 Nh bytes), boxes of up to 256 rows
+            const int bh = (int)std::min<int64_t>(P.ny, 256);
+            ok = encode_view(&tm[0], data, 2 * nh, P.nx * P.ny, 16 * nh, 2 * wy, bh) &&
+                 encode_view(&tm[1], data, 2 * nh, P.nx * P.ny, 16 * nh, 2 * wy, bh) &&
+                 encode_view(&tm[2], data, 2 * nh, P.nx * P.ny, 16 * nh, 2, bh);
+        }
+        if (!ok) return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass A field view");
         q::PassAQParams qp{};
         qp.data = data;
         qp.unp = P.q_unp;
@@ -969,14 +1007,9 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd, do
         prm.wx = P.fb->w;
         prm.ntiles = (prm.ncols + P.fb->w - 1) / P.fb->w;
         CUtensorMap tm;
-        const auto enc = tensor_map_encoder();
-        const cuuint64_t dims[2] = {(cuuint64_t)prm.ncols, (cuuint64_t)P.nx};
-        const cuuint64_t strides[1] = {(cuuint64_t)prm.ncols * 8};
-        const cuuint32_t box[2] = {(cuuint32_t)P.fb->w, (cuuint32_t)std::min<int64_t>(P.nx, 256)};
-        const cuuint32_t es[2] = {1, 1};
-        if (!enc || enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, data, dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        const int epc = (int)sizeof(cx_t<T>) / 8;  // 8-byte elements per complex
+        if (!encode_view(&tm, data, prm.ncols * epc, P.nx, prm.ncols * (long long)sizeof(cx_t<T>), P.fb->w * epc,
+                         (int)std::min<int64_t>(P.nx, 256)))
             return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass B field view");
         void *args[] = {&prm, &tm};
         const void *k = prm.epi ? (fwd ? P.fb->kfwd_epi : P.fb->kinv_epi) : (fwd ? P.fb->kfwd : P.fb->kinv);
