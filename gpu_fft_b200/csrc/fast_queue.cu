@@ -12,22 +12,18 @@ namespace fast {
     {2, NBUF, DT, NY, M, 2, WY, NT + 32, VY, 0, q::QShape<T, NY, M, NT, NBUF, WY>::smem_bytes(),                \
      (const void *)q::pass_a_queue<T, NY, M, NT, true, VY, NBUF, WY>,                                           \
      (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY>, nullptr, nullptr}
-// the same with the y FFT ping-ponging through a scratch tile
-#define QP_ENTRY(T, DT, NY, M, NT, VY, NBUF, WY)                                                                \
-    {2, NBUF, DT, NY, M, 2, WY, NT + 32, VY, 0, q::QShape<T, NY, M, NT, NBUF, WY, true>::smem_bytes(),          \
-     (const void *)q::pass_a_queue<T, NY, M, NT, true, VY, NBUF, WY, true>,                                     \
-     (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY, true>, nullptr, nullptr}
 
 const VariantA kVariantsA_f32q[] = {
     // 512^2 planes, B200, ms per launch at 512^3 (forward / inverse, queue
-    // depth 16-32): 16 consumer warps, 16-column items, 3-deep ring of 72 KB
-    // buffers 0.398 / 0.426; 2-deep 0.412 / 0.435.  Measured and dropped:
-    // 8 consumer warps (16-row items) 0.425 / 0.473, 8-column items with a
-    // 4-deep ring 0.475 / 0.520 (8 warps) and 0.457 / 0.500 (16 warps)
+    // depth 24-32): 16 consumer warps, 16-column items, 3-deep ring of 72 KB
+    // buffers 0.396 / 0.407; 2-deep 0.412 / 0.435.  Measured and dropped:
+    // 8 consumer warps (16-row items) 0.425 / 0.473; 8-column items with a
+    // 4-deep ring 0.475 / 0.520 (8 warps) and 0.457 / 0.500 (16 warps); the y
+    // FFT as 16 x 16 x 2 0.403 / 0.441; the y FFT alternating with a 64 KB
+    // scratch tile (two barriers per item fewer, 2-deep ring) 0.406 / 0.417
     QA_ENTRY(float, 0, 512, 256, 512, 0, 3, 16),
     QA_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
-    QA_ENTRY(float, 0, 512, 256, 512, 1, 3, 16),
-    QP_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
+
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),

@@ -68,7 +68,7 @@ using fast::ToSmem;
 
 struct PassAQParams {
     void *data;
-    const void *unp;    // exp(-2 pi i k / Nz), k < M (the full unpack table)
+    const void *unp;    // unpack / pack factors, k < M: forward -i w^k / 2, inverse i conj(w^k), w = exp(-2 pi i / Nz)
     const void *rtw;    // row FFT step-1 twiddles: exp(-2 pi i a f / M) at (f - 1) * 16 + a, f < M / 16
     const void *sty;    // per-stage table of the y FFT (fft_fast.cuh stage_offset)
     const int *items;   // work list: (plane << 16) | (type << 15) | sub
@@ -160,9 +160,8 @@ __device__ __forceinline__ void group_sync() {
 // FP64: rows are 16-byte aligned on their own; the view is [rows][2 Nh]
 // 8-byte elements and box E is WY columns of every row (NBX boxes of BHT
 // rows), box X the one column M of every row.
-template <typename T, int NY, int M, int NT, int NBUF, int WY_, bool PP_ = false>
+template <typename T, int NY, int M, int NT, int NBUF, int WY_>
 struct QShape {
-    static constexpr bool PP = PP_;  // column FFT ping-pongs with a scratch tile
     using V = cx_t<T>;
     static constexpr bool PAIR = sizeof(V) == 8;
     static constexpr int NH = M + 1;
@@ -185,11 +184,8 @@ struct QShape {
     static constexpr int BUF = rup(mx(mx(ROW_BYTES, TILE_BYTES), X_OFF + X_BYTES));
     static constexpr int R2 = M / 16;                // row FFT: M = 16 x R2
     static constexpr int TAB = rup((M + M + NY) * (int)sizeof(V));
-    static constexpr int PONG = PP ? rup(TILE_BYTES) : 0;
-    // tables, buffers, the scratch tile, mbarriers, slot words, and slack for 128-byte alignment
-    static constexpr size_t smem_bytes() {
-        return (size_t)TAB + (size_t)NBUF * BUF + (size_t)PONG + 2 * NBUF * 8 + NBUF * 4 + 128;
-    }
+    // tables, buffers, mbarriers, slot words, and slack for 128-byte alignment
+    static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + 2 * NBUF * 8 + NBUF * 4 + 128; }
     static_assert(!PAIR || NH % 2 == 1, "row-pair view needs Nh odd (Nz a multiple of 4)");
     static_assert(!PAIR || BH <= 256, "box height");
     static_assert(PAIR || NY % BHT == 0, "whole boxes");
@@ -227,114 +223,13 @@ __device__ __forceinline__ void row_step2(V (&y)[16], const V *row, int b) {
 }
 
 // ---------------------------------------------------------------------------
-// Column tile FFT alternating between two shared buffers (ping-pong): the
-// same Stockham stages as TileFFT (COLS layout, element (n, w) at n W + w),
-// but stage s reads one buffer and writes the other, so a stage needs no
-// barrier between its reads and its writes -- only the one before it reads
-// the previous stage's output.  Stage 0 reads through `src`, the stages
-// alternate P, A, P, ...; the last writes through `dst`, or (ToSmem) into its
-// buffer, which run() returns.
-// ---------------------------------------------------------------------------
-template <typename T, int N, int W, int NT, bool FWD, int VARIANT>
-struct PPFFT {
-    using V = cx_t<T>;
-    static constexpr fast::Fac F = fast::factor(N, VARIANT);
-    static constexpr int NS = F.n;
-    static_assert(NS >= 1, "a length with stages");
-
-    template <int S, class Src, class Dst>
-    static __device__ __forceinline__ void stage(Src &src, Dst &dst, const V *in, V *out, const V *tw) {
-        constexpr int R = F.r[S];
-        constexpr int p = fast::fac_prod(F, S);
-        constexpr int nb = N / R;
-        constexpr int items = nb * W;
-        constexpr int C = (items + NT - 1) / NT;
-        constexpr bool first = S == 0, last = S == NS - 1;
-        constexpr bool to_smem = !last || std::is_same<Dst, ToSmem>::value;
-        const int tid = threadIdx.x;
-        if constexpr (!first) group_sync<NT>();  // the previous stage's output is complete
-        V v[C][R];
-        int ii[C], ww[C];
-#pragma unroll
-        for (int m = 0; m < C; ++m) {
-            const int q = tid + m * NT;
-            ii[m] = q / W;
-            ww[m] = q % W;
-            if ((m + 1) * NT <= items || q < items) {
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    if constexpr (first)
-                        v[m][j] = src(ii[m] + j * nb, ww[m]);
-                    else
-                        v[m][j] = in[(ii[m] + j * nb) * W + ww[m]];
-                }
-            }
-        }
-        // butterflies NT / W apart in i share k = i mod p when that is a multiple of p
-        constexpr bool shared_k = p > 1 && C > 1 && (NT / W) % p == 0 && NT % W == 0;
-        V tws[shared_k ? R : 1];
-        if constexpr (shared_k) {
-            constexpr int off = fast::stage_offset(F, S);
-            const int k0 = ii[0] % p;
-#pragma unroll
-            for (int j = 1; j < R; ++j) tws[j] = tw[off + (j - 1) * p + k0];
-        }
-#pragma unroll
-        for (int m = 0; m < C; ++m) {
-            const int q = tid + m * NT;
-            if ((m + 1) * NT <= items || q < items) {
-                const int i = ii[m], w = ww[m];
-                const int k = i % p;
-                if constexpr (shared_k) {
-#pragma unroll
-                    for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tws[j]);
-                } else if constexpr (p > 1) {
-                    constexpr int off = fast::stage_offset(F, S);
-#pragma unroll
-                    for (int j = 1; j < R; ++j) v[m][j] = c_tw<FWD>(v[m][j], tw[off + (j - 1) * p + k]);
-                }
-                Dft<R, FWD, V>::run(v[m]);
-                if constexpr (last) {
-#pragma unroll
-                    for (int j = 0; j < R; ++j) {
-                        if constexpr (to_smem)
-                            out[(i + j * nb) * W + w] = v[m][j];
-                        else
-                            dst(i + j * nb, w, v[m][j]);
-                    }
-                } else {
-                    const int o = (i - k) * R + k;
-#pragma unroll
-                    for (int j = 0; j < R; ++j) out[(o + j * p) * W + w] = v[m][j];
-                }
-            }
-        }
-    }
-    template <int S, class Src, class Dst>
-    static __device__ __forceinline__ V *stages(Src &src, Dst &dst, V *a, V *pp, const V *tw) {
-        // stage S writes pp when S is even, a when odd
-        V *in = (S % 2 == 0) ? a : pp;
-        V *out = (S % 2 == 0) ? pp : a;
-        stage<S>(src, dst, in, out, tw);
-        if constexpr (S + 1 < NS)
-            return stages<S + 1>(src, dst, a, pp, tw);
-        else
-            return out;
-    }
-    template <class Src, class Dst>
-    static __device__ __forceinline__ V *run(Src &src, Dst &dst, V *a, V *pp, const V *tw) {
-        return stages<0>(src, dst, a, pp, tw);
-    }
-};
-
-// ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
-template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16, bool PP = false>
+template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16>
 __global__ void __launch_bounds__(NT + 32, 1)
     pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
                  const __grid_constant__ CUtensorMap tm_x) {
-    using S = QShape<T, NY, M, NT, NBUF, WY_, PP>;
+    using S = QShape<T, NY, M, NT, NBUF, WY_>;
     using V = cx_t<T>;
     using ColFFT = TileFFT<T, NY, S::WY, NT, FWD, COLS, VY, GROUP>;
     using ColL = typename ColFFT::L;
@@ -346,8 +241,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
     V *rtw = unp + M;
     V *sty = rtw + M;
     unsigned char *bufs = smem + S::TAB;
-    V *pong = reinterpret_cast<V *>(bufs + (size_t)NBUF * S::BUF);  // (PP only)
-    uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF + S::PONG);
+    uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF);
     uint64_t *empty = full + NBUF;
     int *info = reinterpret_cast<int *>(empty + NBUF);
 
@@ -507,20 +401,19 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     }
                     __syncwarp();
                     // unpack: X[k] = E + O, E = (Z[k] + conj Z[M-k]) / 2,
-                    // O = -i w^k (Z[k] - conj Z[M-k]) / 2; bins 0 and M packed in slot 0
+                    // O = -i w^k (Z[k] - conj Z[M-k]) / 2 = (Z[k] - conj Z[M-k]) u_k with
+                    // the table u_k = -i w^k / 2; bins 0 and M packed in slot 0
                     const T hf = (T)0.5;
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
                         const int kk = a + 16 * j;
                         const V za = R2 == 16 ? x[j] : row[kk];
                         const V zb = c_conj(row[(kk == 0 ? 0 : M - kk)]);
-                        const V e = c_scale(c_add(za, zb), hf);
-                        const V d = c_scale(c_sub(za, zb), hf);
-                        const V o = c_rot<true>(c_mul(d, unp[kk]));
-                        const V xa = c_add(e, o);
+                        const V e2 = c_add(za, zb);
+                        const V o = c_mul(c_sub(za, zb), unp[kk]);
+                        const V xa = V{fma(hf, e2.x, o.x), fma(hf, e2.y, o.y)};
                         if (kk == 0) {
-                            const V xb = c_conj(c_sub(e, o));
-                            st_g(grow, V{xa.x, xb.x});
+                            st_g(grow, V{xa.x, fma(hf, e2.x, -o.x)});  // (Re X0, Re XM)
                         } else {
                             st_g(grow + kk, xa);
                         }
@@ -536,10 +429,9 @@ __global__ void __launch_bounds__(NT + 32, 1)
                             xb = V{xa.y, (T)0};
                             xa = V{xa.x, (T)0};
                         }
+                        // (the table holds i conj(w^k))
                         const V cm = c_conj(xb);
-                        const V sv = c_add(xa, cm);
-                        const V pk = c_rot<false>(c_mulc(c_sub(xa, cm), unp[kk]));
-                        x[j] = c_add(sv, pk);
+                        x[j] = c_add(c_add(xa, cm), c_mul(c_sub(xa, cm), unp[kk]));
                     }
                     row_step1<false, R2>(x, row, rtw, a);
                     if (R2 == 16 || a < R2) {
@@ -558,21 +450,21 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 const V *bx = reinterpret_cast<const V *>(b + S::X_OFF);
                 V *tile = reinterpret_cast<V *>(b);
                 auto at = [&](int n, int w) -> V {
-                    if constexpr (S::PAIR)
-                        return (n & 1) ? bo[(n >> 1) * (WY + 2) + 1 + w] : be[(n >> 1) * WY + w];
-                    else
+                    if constexpr (S::PAIR) {
+                        // one load path for both parities (an integer select, no
+                        // branch): half-warps hold rows of opposite parity
+                        const int h = n >> 1;
+                        const int off = (n & 1) ? S::O_OFF / (int)sizeof(V) + h * (WY + 2) + 1 : h * WY;
+                        return be[off + w];
+                    } else {
                         return be[n * WY + w];
+                    }
                 };
                 auto dst = [&](int n, int w, V v) { st_g(gplane + (long long)n * NH + c0 + w, v); };
-                // the y FFT in place in the buffer, or alternating with the
-                // scratch tile (PP); returns where a ToSmem result lies
+                // the y FFT in place in the buffer; returns where a ToSmem result lies
                 auto colfft = [&](auto &src_, auto &dst_) -> V * {
-                    if constexpr (PP) {
-                        return PPFFT<T, NY, WY, NT, FWD, VY>::run(src_, dst_, tile, pong, sty);
-                    } else {
-                        ColFFT::run(src_, dst_, tile, sty);
-                        return tile;
-                    }
+                    ColFFT::run(src_, dst_, tile, sty);
+                    return tile;
                 };
                 if constexpr (FWD) {
                     auto src = [&](int n, int w) -> V { return at(n, w); };

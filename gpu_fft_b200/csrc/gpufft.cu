@@ -272,6 +272,7 @@ static void free_queue(Plan &P) {
     P.q_dev = nullptr;
     P.q_items_f = P.q_items_i = nullptr;
     P.q_unp = nullptr;
+    P.q_unp_i = nullptr;
     P.q_rtw = nullptr;
 }
 
@@ -312,20 +313,24 @@ static int setup_queue(Plan &P) {
     depth = std::max(1, std::min(nx, depth));
     const std::vector<int> fwd = queue_items(nx, nri, nci, q::ROW_ITEM, depth);
     const std::vector<int> inv = queue_items(nx, nci, nri, q::COL_ITEM, depth);
-    // unpack roots exp(-2 pi i k / Nz), k < M, then the row FFT's step-1
-    // twiddles exp(-2 pi i a f / M) at (f - 1) * 16 + a (M = 16 * R2): FP64-class
-    // host values rounded once
+    // the unpack factors u_k = -i w^k / 2 (forward) and the pack factors
+    // v_k = i conj(w^k) (inverse), w = exp(-2 pi i / Nz), k < M; then the row
+    // FFT's step-1 twiddles exp(-2 pi i a f / M) at (f - 1) * 16 + a
+    // (M = 16 * R2): long-double host values rounded once
     const int r2 = m / 16;
-    std::vector<double> unp(2 * (size_t)m + 2 * 16 * (size_t)std::max(r2 - 1, 0));
+    std::vector<double> unp(4 * (size_t)m + 2 * 16 * (size_t)std::max(r2 - 1, 0));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int k = 0; k < m; ++k) {
         const long double ang = two_pi * (long double)k / (long double)(2 * m);
-        unp[2 * k] = (double)cosl(ang);
-        unp[2 * k + 1] = (double)(-sinl(ang));
+        const long double c = cosl(ang), sn = sinl(ang);  // w^k = c - i sn
+        unp[2 * k] = (double)(-sn / 2);                   // -i w^k / 2
+        unp[2 * k + 1] = (double)(-c / 2);
+        unp[2 * m + 2 * k] = (double)(-sn);               // i conj(w^k)
+        unp[2 * m + 2 * k + 1] = (double)c;
     }
     for (int f = 1; f < r2; ++f)
         for (int a = 0; a < 16; ++a) {
-            const size_t at = 2 * (size_t)m + 2 * ((size_t)(f - 1) * 16 + a);
+            const size_t at = 4 * (size_t)m + 2 * ((size_t)(f - 1) * 16 + a);
             const long double ang = two_pi * (long double)((a * f) % m) / (long double)m;
             unp[at] = (double)cosl(ang);
             unp[at + 1] = (double)(-sinl(ang));
@@ -364,7 +369,8 @@ static int setup_queue(Plan &P) {
     P.q_items_f = reinterpret_cast<const int *>(b + cbytes);
     P.q_items_i = reinterpret_cast<const int *>(b + cbytes + lbytes);
     P.q_unp = b + cbytes + 2 * lbytes;
-    P.q_rtw = b + cbytes + 2 * lbytes + 2 * (size_t)m * tsz;
+    P.q_unp_i = b + cbytes + 2 * lbytes + 2 * (size_t)m * tsz;
+    P.q_rtw = b + cbytes + 2 * lbytes + 4 * (size_t)m * tsz;
     return GPUFFT_SUCCESS;
 }
 
@@ -929,7 +935,7 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
         if (!ok) return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass A field view");
         q::PassAQParams qp{};
         qp.data = data;
-        qp.unp = P.q_unp;
+        qp.unp = fwd ? P.q_unp : P.q_unp_i;
         qp.rtw = P.q_rtw;
         qp.sty = P.pa.sty;
         qp.items = fwd ? P.q_items_f : P.q_items_i;

@@ -39,7 +39,8 @@ struct Plan {
     int q_nitems = 0;    // items per launch
     int q_need = 0;      // first-phase items per plane (forward)
     const int *q_items_f = nullptr, *q_items_i = nullptr;
-    const void *q_unp = nullptr;
+    const void *q_unp = nullptr;    // forward unpack factors
+    const void *q_unp_i = nullptr;  // inverse pack factors
     const void *q_rtw = nullptr;  // the row FFT's step-1 twiddles
 };
 
