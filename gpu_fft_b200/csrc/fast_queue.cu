@@ -20,7 +20,10 @@ const VariantA kVariantsA_f32q[] = {
     // 8 consumer warps (16-row items) 0.425 / 0.473; 8-column items with a
     // 4-deep ring 0.475 / 0.520 (8 warps) and 0.457 / 0.500 (16 warps); the y
     // FFT as 16 x 16 x 2 0.403 / 0.441; the y FFT alternating with a 64 KB
-    // scratch tile (two barriers per item fewer, 2-deep ring) 0.406 / 0.417
+    // scratch tile (two barriers per item fewer, 2-deep ring) 0.406 / 0.417;
+    // two groups of 8 consumer warps, each on its own 16-row or 8-column
+    // items (barrier waits of one group overlapping the other's work), 4- or
+    // 5-deep ring of 40 KB buffers 0.467-0.476 / 0.484-0.492
     QA_ENTRY(float, 0, 512, 256, 512, 0, 3, 16),
     QA_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
 
