@@ -27,7 +27,7 @@ STATUS = {0: "SUCCESS", 1: "ERR_INVALID", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4
 # every symbol include/gpufft_b200.h declares
 EXPORTS = (
     "gpufft_init", "gpufft_r2c", "gpufft_c2r", "gpufft_finalize", "gpufft_last_error",
-    "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_exec_r2c", "gpufft_exec_c2r",
+    "gpufft_plan_create", "gpufft_plan_destroy", "gpufft_plan_check", "gpufft_exec_r2c", "gpufft_exec_c2r",
     "gpufft_exec_pass", "gpufft_exec_r2c_ex", "gpufft_exec_c2r_ex", "gpufft_field_bytes", "gpufft_plan_launches", "gpufft_plan_describe",
     "gpufft_plan_create_ex", "gpufft_plan_autotune", "gpufft_wisdom_save", "gpufft_wisdom_load",
     "gpufft_exec_noalloc",
@@ -86,6 +86,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gpufft_last_error.restype = ctypes.c_char_p
     lib.gpufft_plan_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, ci]
     lib.gpufft_plan_destroy.argtypes = [vp]
+    lib.gpufft_plan_check.argtypes = [vp]
     lib.gpufft_exec_r2c.argtypes = [vp, vp, vp]
     lib.gpufft_exec_c2r.argtypes = [vp, vp, vp]
     lib.gpufft_exec_pass.argtypes = [vp, vp, vp, ci, ci]
@@ -258,6 +259,11 @@ class Plan:
         buf = ctypes.create_string_buffer(1024)
         load_library().gpufft_plan_describe(self._h, buf, 1024)
         return buf.value.decode()
+
+    def check(self) -> None:
+        """Raises GpuFFTError (ERR_CUDA) if a bounded wait inside one of the
+        plan's kernels ran out (gpufft_plan_check; synchronous)."""
+        _check(load_library().gpufft_plan_check(self._h))
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -52,6 +52,9 @@ const VariantB kVariantsB_f32q[] = {
     TB_ENTRY(float, 0, 512, 256, 0, 2),
     TB_ENTRY(float, 0, 512, 256, 1, 3),
     TB_ENTRY(float, 0, 512, 512, 1, 3),
+    // radix-16 stages on tcgen05 (v = 3, fft_tc5.cuh): only plans made with
+    // GPUFFT_PLAN_TC_SPLIT use it
+    TB_ENTRY(float, 0, 512, 512, 3, 2),
     // (Nx = 1024, one 128 KB tile buffer refilled during the last stage by
     // tensor copies: 0.226 ms per launch at 1024x512x256 against 0.222 for
     // the same scheme with cp.async, pass_b_pipe1 -- not registered)

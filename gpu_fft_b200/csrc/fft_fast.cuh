@@ -20,6 +20,7 @@
 
 #include "fft_kernels.cuh"
 #include "fft_radix.cuh"
+#include "fft_tc5.cuh"
 
 namespace gpufft {
 namespace fast {
@@ -182,6 +183,11 @@ struct TileFFT {
     static constexpr bool kTcStage = VARIANT == 2 && std::is_same<T, float>::value && LAYOUT == COLS &&
                                      SCOPE == BLOCK && W == 16 && NT >= 64 && (N & (N - 1)) == 0 &&
                                      (NT & (NT - 1)) == 0;
+    // VARIANT 3: the radix-16 stages but the last on tcgen05 (fft_tc5.cuh):
+    // FP32 column tiles of width 16 read from shared memory, whole CTA, one
+    // butterfly per thread, NT / 128 blocks of 128 butterflies
+    static constexpr bool kTc5Stage = VARIANT == 3 && std::is_same<T, float>::value && LAYOUT == COLS &&
+                                      SCOPE == BLOCK && W == 16 && NT % 128 == 0 && NT / 128 <= tc5::kMaxBlocks;
     using L = TileLayout<T, N, W, LAYOUT, kTcStage>;
     static constexpr Fac F = factor(N, VARIANT);
     static constexpr int NS = F.n;
@@ -369,6 +375,69 @@ struct TileFFT {
             }
         }
     }
+    // ---- radix-16 stage on tcgen05 (VARIANT 3).  Thread t takes butterfly
+    // (i, w) = (t / W, t % W): it reads its 16 inputs, applies the stage's
+    // twiddles, writes the TF32 split operands to its tensor-memory lane,
+    // and after the block barrier and the MMAs (issued by thread 0) reads
+    // its 16 outputs back and stores them to the tile.
+    template <int S>
+    static __device__ __forceinline__ void stage_tc5(V *sm, const V *tw) {
+        constexpr int R = 16;
+        constexpr int p = fac_prod(F, S);
+        constexpr int nb = N / R;
+        static_assert(nb * W == NT, "one butterfly per thread");
+        static_assert(S < NS - 1, "the last stage runs on the FP32 pipes");
+        tc5::State &ts = tc5::state();
+        const int tid = threadIdx.x, warp = tid >> 5;
+        const int w = tid % W, i = tid / W, k = i % p;
+        V v[R];
+        sync();  // the previous writer of the tile is done
+        const uint32_t par = ts.phase & 1u;  // (advanced by thread 0 after the next barrier)
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = sm[L::idx_sum(i, j * nb, w)];
+        if constexpr (p > 1) {
+            constexpr int off = stage_offset(F, S);
+#pragma unroll
+            for (int j = 1; j < R; ++j) v[j] = c_tw<FWD>(v[j], tw[off + (j - 1) * p + k]);
+        }
+        // this thread's lane of its block's columns: Xh = [Re | Im] at 0-31, Xl at 32-63, Y at 64-95
+        const uint32_t taddr = ts.tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * tc5::kColsPerBlock);
+        {
+            uint32_t h[16], l[16];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                h[j] = tc5::rna_tf32(v[j].x);
+                l[j] = __float_as_uint(v[j].x - __uint_as_float(h[j]));
+            }
+            tc5::st16(taddr, h);
+            tc5::st16(taddr + 32, l);
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                h[j] = tc5::rna_tf32(v[j].y);
+                l[j] = __float_as_uint(v[j].y - __uint_as_float(h[j]));
+            }
+            tc5::st16(taddr + 16, h);
+            tc5::st16(taddr + 48, l);
+        }
+        tc5::wait_st();
+        tc5::fence_before();
+        sync();  // every operand is in tensor memory and every input of the tile has been read
+        if (tid == 0) {
+            tc5::issue(NT / 128);
+            ts.phase += 1;
+        }
+        if (!tc5::bar_wait(&ts.bar, par)) ts.err = 1;
+        tc5::fence_after();
+        uint32_t d[32];
+        tc5::ld32(taddr + 64, d);
+        tc5::wait_ld();
+        tc5::fence_before();  // these reads precede the next MMAs (after a barrier)
+        // outputs at rows o + j p, o = (i - k) R + k
+        const int o = (i - k) * R + k;
+#pragma unroll
+        for (int j = 0; j < R; ++j) sm[L::idx_sum(o, j * p, w)] = V{__uint_as_float(d[j]), __uint_as_float(d[16 + j])};
+    }
+
     // two adjacent complex values at an even tile index (16-byte aligned)
     static __device__ __forceinline__ void st_pair(V *sm, int idx, V a, V b) {
         *reinterpret_cast<float4 *>(sm + idx) = make_float4(a.x, a.y, b.x, b.y);
@@ -378,6 +447,11 @@ struct TileFFT {
     static __device__ __forceinline__ void stage(Src &src, Dst &dst, V *sm, const V *tw, Hook &hook) {
         if constexpr (kTcStage && F.r[S] == 16 && S < NS - 1) {
             stage_tc16<S>(src, dst, sm, tw);
+            return;
+        } else if constexpr (kTc5Stage && F.r[S] == 16 && S < NS - 1) {
+            static_assert(S != 0 || std::is_same<Src, FromSmem>::value,
+                          "the tcgen05 stages read the tile from shared memory");
+            stage_tc5<S>(sm, tw);
             return;
         } else {
             stage_scalar<S>(src, dst, sm, tw, hook);

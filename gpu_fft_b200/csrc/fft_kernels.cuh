@@ -100,6 +100,7 @@ struct PassBParams {
     int epi, dealias;
     double scale;
     int ny, nh, nz;
+    int *err;  // device flag raised by a kernel whose bounded wait ran out (or null)
 };
 
 // the x pass's store of value v at (kx, column), with the epilogue applied

@@ -544,6 +544,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
 // NBUF = 1 (tiles too large for two buffers: Nx = 1024) refills the one
 // buffer as soon as the last FFT stage has read it (TileFFT::run's hook),
 // so the next tile streams in while that stage computes and stores.
+// VARIANT 3 runs the radix-16 stages but the last on tcgen05 (fft_tc5.cuh):
+// the CTA holds the whole tensor memory; if a wait for the MMAs runs out
+// (2 s), the CTA stops, waits for its copies still in flight (bounded),
+// frees the tensor memory and raises P.err.
 // ---------------------------------------------------------------------------
 template <typename T, int NX, int NT, int NBUF>
 struct BShape {
@@ -572,6 +576,8 @@ __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const _
     unsigned char *bufs = smem + S::TAB;
     uint64_t *full = reinterpret_cast<uint64_t *>(bufs + (size_t)NBUF * S::BUF);
     for (int q = threadIdx.x; q < NX - 1; q += NT) tw[q] = reinterpret_cast<const V *>(P.stw)[q];
+    constexpr bool TC5 = FFT::kTc5Stage;
+    if constexpr (TC5) tc5::setup<FWD>();
     auto issue = [&](long long t, int s) {
         unsigned char *b = bufs + (size_t)s * S::BUF;
         mbar_arrive_expect_tx(&full[s], (uint32_t)S::TILE_BYTES);
@@ -621,6 +627,7 @@ __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const _
                 }
             };
             FFT::run(fs, dst, tile, tw, refill);
+            if constexpr (TC5) __syncthreads();
         } else {
             FFT::run(fs, dst, tile, tw);
             __syncthreads();  // every read of the tile is done: refill its buffer
@@ -629,7 +636,22 @@ __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const _
                 issue(tn, s);
             }
         }
+        if constexpr (TC5) {
+            if (tc5::state().err) {
+                // copies of the next NBUF tiles may be in flight: wait for them
+                if (threadIdx.x == 0) {
+                    for (int e = 1; e <= NBUF; ++e) {
+                        if (t + (long long)e * gridDim.x >= P.ntiles) break;
+                        const int k2 = k + e;
+                        mbar_wait(&full[k2 % NBUF], (uint32_t)((k2 / NBUF) & 1), 2000000000LL);
+                    }
+                    if (P.err) atomicExch(P.err, 1);
+                }
+                break;
+            }
+        }
     }
+    if constexpr (TC5) tc5::teardown();
 }
 
 }  // namespace q

@@ -254,13 +254,13 @@ static const std::vector<fast::VariantB> &variants_b(int dtype) {
 }
 
 // A Pass B entry serves this plan: its length, 16-byte tile rows for the
-// cp.async form, and tensor-core stages (v = 2) exactly when the plan asks
-// for them.
+// cp.async and tensor-copy forms, and tensor-core stages (v = 2: mma.sync,
+// v = 3: tcgen05) exactly when the plan asks for them.
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 static bool b_eligible(const Plan &P, const fast::VariantB &v) {
     const int m = (int)(P.nz / 2);
     const bool rows16 = ((long long)P.ny * (m + 1) * (P.dtype == GPUFFT_FLOAT ? 8 : 16)) % 16 == 0;
-    return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v == 2) == P.tc_split) &&
+    return v.nx == (int)P.nx && (v.kind == 0 || rows16) && ((v.v >= 2) == P.tc_split) &&
            (v.kind != 3 || tensor_map_encoder());
 }
 
@@ -779,14 +779,18 @@ static int build_plan(Plan &P) {
     // ---- twiddle tables on the device
     const std::vector<T> hx = twiddle_table<T>(nx), hy = twiddle_table<T>(ny), hz = twiddle_table<T>(nz);
     const size_t bx = hx.size() * sizeof(T), by = hy.size() * sizeof(T), bz = hz.size() * sizeof(T);
-    cudaError_t e = cudaMalloc(&P.tw_dev, bx + by + bz);
+    // (then 16 bytes of device flags: [0] a tensor-core x pass's bounded wait ran out)
+    const size_t fl = (bx + by + bz + 15) / 16 * 16;
+    cudaError_t e = cudaMalloc(&P.tw_dev, fl + 16);
     if (e != cudaSuccess) return set_error(GPUFFT_ERR_OOM, "cudaMalloc twiddles: %s", cudaGetErrorString(e));
     char *base = (char *)P.tw_dev;
-    e = cudaMemcpy(base, hx.data(), bx, cudaMemcpyHostToDevice);
+    e = cudaMemset(base + fl, 0, 16);
+    if (e == cudaSuccess) e = cudaMemcpy(base, hx.data(), bx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(base + bx, hy.data(), by, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(base + bx + by, hz.data(), bz, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemcpy twiddles");
     B.twx = base;
+    B.err = reinterpret_cast<int *>(base + fl);
     A.twy = base + bx;
     A.twz = base + bx + by;
 
@@ -1264,6 +1268,23 @@ extern "C" int gpufft_wisdom_load(const char *path) {
 }
 
 extern "C" int gpufft_plan_destroy(gpufft_plan plan) { return plan_destroy(reinterpret_cast<Plan *>(plan)); }
+
+extern "C" int gpufft_plan_check(gpufft_plan plan) {
+    Plan *P = reinterpret_cast<Plan *>(plan);
+    if (!P || !P->tw_dev) return set_error(GPUFFT_ERR_NOT_INIT, "no plan");
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != P->device) cudaSetDevice(P->device);
+    int tc = 0, qe = 0;
+    cudaError_t e = cudaMemcpy(&tc, P->pb.err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && P->q_dev) e = cudaMemcpy(&qe, reinterpret_cast<int *>(P->q_dev) + 2, sizeof(int), cudaMemcpyDeviceToHost);
+    if (cur != P->device && cur >= 0) cudaSetDevice(cur);
+    if (e != cudaSuccess) return cuda_error(e, "read the plan's device flags");
+    if (tc || qe)
+        return set_error(GPUFFT_ERR_CUDA, "a bounded device-side wait of this plan's kernels ran out (%s%s%s)",
+                         qe ? "queue Pass A" : "", qe && tc ? ", " : "", tc ? "tensor-core x pass" : "");
+    return GPUFFT_SUCCESS;
+}
 
 extern "C" int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream) {
     return plan_exec(reinterpret_cast<Plan *>(plan), data, stream, true);

@@ -91,6 +91,12 @@ const char *gpufft_last_error(void);
  * ------------------------------------------------------------------------ */
 int gpufft_plan_create(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype);
 int gpufft_plan_destroy(gpufft_plan plan);
+/* Reads the plan's device-side error flags (synchronous): GPUFFT_ERR_CUDA if
+ * a bounded wait inside one of its kernels ran out since the plan was made
+ * (the queue-scheduled Pass A waiting for a plane, or the tensor-core x pass
+ * waiting for its MMAs; the results of that call are wrong and the plan
+ * should be destroyed), else GPUFFT_SUCCESS.  No reference counterpart. */
+int gpufft_plan_check(gpufft_plan plan);
 int gpufft_exec_r2c(gpufft_plan plan, void *data, void *stream);
 int gpufft_exec_c2r(gpufft_plan plan, void *data, void *stream);
 /* The same with an epilogue fused into the x pass, for pseudo-spectral steps
@@ -124,11 +130,13 @@ int gpufft_exec_pass(gpufft_plan plan, void *data, void *stream, int pass, int f
  * ------------------------------------------------------------------------ */
 #define GPUFFT_PLAN_AUTOTUNE 1
 /* FP32 plans only: the x pass runs its radix-16 stages as 16x16 DFT-matrix
- * products on the tensor cores (mma.sync, BF16 operands split into three
- * terms, FP32 accumulation; within about 1e-7 relative L2 of the plain FP32
- * plan).  Compiled for Nx = 512 and 1024; other Nx give
- * GPUFFT_ERR_UNSUPPORTED.  No reference counterpart (GPU_FFT's transforms
- * are cuFFT's). */
+ * products on the tensor cores, in one of two forms (the autotuner picks):
+ * tcgen05.mma with TF32 operands split into two terms (three products) and
+ * FP32 accumulators in tensor memory (Nx = 512, 16-byte-aligned rows), or
+ * mma.sync with BF16 operands split into three terms (six products).  Both
+ * stay within about 1e-7 relative L2 of the plain FP32 plan.  Compiled for
+ * Nx = 512 and 1024; other Nx give GPUFFT_ERR_UNSUPPORTED.  No reference
+ * counterpart (GPU_FFT's transforms are cuFFT's). */
 #define GPUFFT_PLAN_TC_SPLIT 2
 
 int gpufft_plan_create_ex(gpufft_plan *plan, int64_t nx, int64_t ny, int64_t nz, int dtype, int flags);

@@ -1,6 +1,8 @@
 """GPU tests of the tensor-core x pass (GPUFFT_PLAN_TC_SPLIT): the radix-16
-stages of the x-axis FFT run as 16x16 DFT-matrix products on mma.sync with
-BF16 operands split into three terms and FP32 accumulation.
+stages of the x-axis FFT run as 16x16 DFT-matrix products on the tensor
+cores -- tcgen05.mma with TF32 operands split into two terms and FP32
+accumulators in tensor memory (v=3), or mma.sync with BF16 operands split
+into three terms and FP32 accumulation (v=2).  Every candidate is tested.
 
 Bars: within 1e-6 relative L2 of the plain FP32 plan on the same input (the
 tensor-core form against the plain one), and within the FP32 bar, 2e-6, of
@@ -31,6 +33,10 @@ def _rel(a, b):
     return float(((a.double() - b.double()).norm() / b.double().norm()).item())
 
 
+def _is_tc(desc):
+    return " v=2 " in desc or " v=3 " in desc
+
+
 def _n_candidates(grid):
     """How many tensor-core x-pass kernels serve this grid (autotune candidates)."""
     import gpu_fft_b200 as g
@@ -44,7 +50,7 @@ def _n_candidates(grid):
             break
         finally:
             os.environ.pop("GPUFFT_VARIANT_B", None)
-        if "v=2" not in p.describe():
+        if not _is_tc(p.describe()):
             break
         n += 1
     return n
@@ -76,7 +82,7 @@ def test_tc_split_matches_plain_fp32_and_oracle(oracle, cuda, grid):
             tc = g.Plan(nx, ny, nz, "float", tc_split=True)
         finally:
             os.environ.pop("GPUFFT_VARIANT_B", None)
-        assert "v=2" in tc.describe()
+        assert _is_tc(tc.describe())
         out = f.clone()
         tc.r2c(out)
         torch.cuda.synchronize()
@@ -116,6 +122,30 @@ def test_tc_split_repeats_bitwise_and_takes_the_epilogue(cuda):
     assert torch.equal(s, a * 0.5)
 
 
+def test_tcgen05_form_is_a_candidate_and_reports_no_wait_timeout(cuda):
+    """At 512 x 48 x 40 (16-byte rows) the tcgen05 x pass is among the
+    candidates; after a transform its device flag is clear."""
+    import torch
+    import gpu_fft_b200 as g
+
+    grid = (512, 48, 40)
+    forms = set()
+    for c in range(_n_candidates(grid)):
+        os.environ["GPUFFT_VARIANT_B"] = str(c)
+        try:
+            p = g.Plan(*grid, "float", tc_split=True)
+        finally:
+            os.environ.pop("GPUFFT_VARIANT_B", None)
+        d = p.describe()
+        forms.add("v=3" if " v=3 " in d else "v=2")
+        f = _field(grid, c)
+        p.r2c(f)
+        p.c2r(f)
+        torch.cuda.synchronize()
+        p.check()
+    assert forms == {"v=2", "v=3"}, forms
+
+
 def test_tc_split_refuses_what_it_does_not_compile(cuda):
     import gpu_fft_b200 as g
 
@@ -127,4 +157,4 @@ def test_tc_split_refuses_what_it_does_not_compile(cuda):
     assert e.value.code == 2
     assert "tensor-core" in str(e.value)
     # a plain plan of the same grid never picks a tensor-core kernel
-    assert "v=2" not in g.Plan(512, 8, 8, "float").describe()
+    assert not _is_tc(g.Plan(512, 8, 8, "float").describe())
