@@ -53,7 +53,9 @@ const VariantB kVariantsB_f32q[] = {
     TB_ENTRY(float, 0, 512, 256, 1, 3),
     TB_ENTRY(float, 0, 512, 512, 1, 3),
     // radix-16 stages on tcgen05 (v = 3, fft_tc5.cuh): only plans made with
-    // GPUFFT_PLAN_TC_SPLIT use it
+    // GPUFFT_PLAN_TC_SPLIT use it.  512^3: 0.360 / 0.360 ms, 1.8e-7 from the
+    // plain pass (mma.sync forms 0.427-0.503 ms).  Fusing Xh [Bh | Bl] into
+    // N = 64 MMAs with per-block barriers: 0.374 ms and 3.8e-7, not kept.
     TB_ENTRY(float, 0, 512, 512, 3, 2),
     // (Nx = 1024, one 128 KB tile buffer refilled during the last stage by
     // tensor copies: 0.226 ms per launch at 1024x512x256 against 0.222 for
