@@ -68,6 +68,12 @@ const int kNumVariantsB_f32q = sizeof(kVariantsB_f32q) / sizeof(kVariantsB_f32q[
 // 72 KB buffers and the 16 KB of tables do not fit)
 const VariantA kVariantsA_f64q[] = {
     QA_ENTRY(double, 1, 512, 256, 256, 0, 2, 8),
+    // 512 x 128 planes (1024 x 512 x 256): two 74 KB buffers
+    QA_ENTRY(double, 1, 512, 128, 256, 0, 2, 8),
+    // 360 x 240 planes (384 x 360 x 480): 12-row items on 6 consumer warps,
+    // two boxes of 180 rows per column item, 2- or 3-deep ring of 51 KB buffers
+    QA_ENTRY(double, 1, 360, 240, 192, 0, 3, 8),
+    QA_ENTRY(double, 1, 360, 240, 192, 0, 2, 8),
 };
 const int kNumVariantsA_f64q = sizeof(kVariantsA_f64q) / sizeof(kVariantsA_f64q[0]);
 

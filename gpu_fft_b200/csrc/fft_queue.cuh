@@ -153,6 +153,14 @@ __device__ __forceinline__ void group_sync() {
     asm volatile("bar.sync 1, %0;\n" ::"n"(N) : "memory");
 }
 
+// Rows per tensor copy of the single-row view: the plane's rows in the fewest
+// equal boxes of at most 256 rows (a tensor-copy box dimension is <= 256).
+__host__ __device__ constexpr int box_rows(int ny) {
+    int k = 1;
+    while (ny / k > 256 || ny % k != 0) ++k;
+    return ny / k;
+}
+
 // ---------------------------------------------------------------------------
 // shape of one instantiation
 // ---------------------------------------------------------------------------
@@ -168,7 +176,7 @@ struct QShape {
     static constexpr int WY = WY_;                   // columns per column item
     static constexpr int RI = NT / 16;               // rows per row item (two per consumer warp)
     static constexpr int BH = NY / 2;                // row pairs per box (PAIR)
-    static constexpr int BHT = NY > 256 ? 256 : NY;  // rows per box (FP64)
+    static constexpr int BHT = box_rows(NY);         // rows per box (FP64)
     static constexpr int NBX = NY / BHT;
     static constexpr int NRI = NY / RI;
     static constexpr int NCI = M / WY;
@@ -181,7 +189,11 @@ struct QShape {
     static constexpr int mx(int a, int b) { return a > b ? a : b; }
     static constexpr int O_OFF = rup(E_BYTES);
     static constexpr int X_OFF = O_OFF + rup(O_BYTES);
-    static constexpr int BUF = rup(mx(mx(ROW_BYTES, TILE_BYTES), X_OFF + X_BYTES));
+    // FP64: box X of every BHT rows lands at a 128-byte pitch (tensor-copy
+    // destinations are 128-byte aligned); XP is that pitch in complex values
+    static constexpr int XB = PAIR ? X_BYTES : rup(BHT * (int)sizeof(V));
+    static constexpr int XP = XB / (int)sizeof(V);
+    static constexpr int BUF = rup(mx(mx(ROW_BYTES, TILE_BYTES), X_OFF + (PAIR ? X_BYTES : NBX * XB)));
     static constexpr int R2 = M / 16;                // row FFT: M = 16 x R2
     static constexpr int TAB = rup((M + M + NY) * (int)sizeof(V));
     // tables, buffers, mbarriers, slot words, and slack for 128-byte alignment
@@ -194,6 +206,9 @@ struct QShape {
     static_assert(M % 16 == 0 && (R2 == 8 || R2 == 15 || R2 == 16), "the row FFT is 16 x 8, 16 x 15 or 16 x 16");
     static_assert(NT % 32 == 0 && NT == 16 * RI, "two rows per consumer warp");
     static_assert(!PAIR || WY % 2 == 0, "16-byte box rows");
+    // every tensor-copy destination is 128-byte aligned: the buffers, O_OFF,
+    // X_OFF and XB by rounding; the FP64 E boxes of BHT rows by this
+    static_assert(PAIR || (BHT * WY * (int)sizeof(V)) % 128 == 0, "128-byte aligned E boxes");
 };
 
 // ---------------------------------------------------------------------------
@@ -349,7 +364,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                             const int y = plane * NY + q * S::BHT;
                             tensor_load_2d(b + (size_t)q * S::BHT * WY * sizeof(V), &tm_e, EPC * c0, y, &full[s]);
                             if (xtra)
-                                tensor_load_2d(b + S::X_OFF + (size_t)q * S::BHT * sizeof(V), &tm_x, EPC * M, y,
+                                tensor_load_2d(b + S::X_OFF + (size_t)q * S::XB, &tm_x, EPC * M, y,
                                                &full[s]);
                         }
                     }
@@ -497,7 +512,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         if constexpr (S::PAIR)
                             return (n & 1) ? bx[(n >> 1) * 2 + 1] : bo[(n >> 1) * (WY + 2)];
                         else
-                            return bx[n];
+                            return bx[(n / S::BHT) * S::XP + n % S::BHT];
                     };
                     auto src = [&](int n, int w) -> V {
                         if (sub == 0 && w == 0) {

@@ -930,8 +930,8 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
             ok = encode_pair_map(&tm[0], data, nh, lines, wy, bh) && encode_pair_map(&tm[1], data, nh, lines, wy + 2, bh) &&
                  encode_pair_map(&tm[2], data, nh, lines, 2, bh);
         } else {
-            // single rows: 2 Nh 8-byte elements per row (16 Nh bytes), boxes of up to 256 rows
-            const int bh = (int)std::min<int64_t>(P.ny, 256);
+            // single rows: 2 Nh 8-byte elements per row (16 Nh bytes), equal boxes of up to 256 rows
+            const int bh = q::box_rows((int)P.ny);
             ok = encode_view(&tm[0], data, 2 * nh, P.nx * P.ny, 16 * nh, 2 * wy, bh) &&
                  encode_view(&tm[1], data, 2 * nh, P.nx * P.ny, 16 * nh, 2 * wy, bh) &&
                  encode_view(&tm[2], data, 2 * nh, P.nx * P.ny, 16 * nh, 2, bh);
