@@ -31,8 +31,13 @@ const VariantA kVariantsA_f32q[] = {
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),
     // 360 x 240 planes (384 x 360 x 480): the row FFT is 16 x 15 (prime-factor
-    // radix 15), 24-row items on 12 consumer warps, 4-deep ring of 52 KB buffers
+    // radix 15), 4-deep ring of 52 KB buffers; ms per launch: 20-row items on
+    // 10 consumer warps 0.230 / 0.235 (an 11-warp CTA gets 168 registers a
+    // thread), 24-row items on 12 warps 0.270 / 0.224 (13 warps get 128 and
+    // the forward spills), 18-row items on 9 warps 0.236 / 0.245
+    QA_ENTRY(float, 0, 360, 240, 320, 0, 4, 16),
     QA_ENTRY(float, 0, 360, 240, 384, 0, 4, 16),
+    QA_ENTRY(float, 0, 360, 240, 288, 0, 4, 16),
 };
 const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[0]);
 
@@ -57,6 +62,12 @@ const VariantB kVariantsB_f32q[] = {
     // plain pass (mma.sync forms 0.427-0.503 ms).  Fusing Xh [Bh | Bl] into
     // N = 64 MMAs with per-block barriers: 0.374 ms and 3.8e-7, not kept.
     TB_ENTRY(float, 0, 512, 512, 3, 2),
+    // Nx = 384 (384 x 360 x 480): two boxes of 192 rows per tile; ms per
+    // launch: 3-deep ring 0.0945, 2-deep 0.103 (256 or 512 threads), against
+    // 0.108 for the cp.async double buffer
+    TB_ENTRY(float, 0, 384, 256, 0, 3),
+    TB_ENTRY(float, 0, 384, 256, 0, 2),
+    TB_ENTRY(float, 0, 384, 512, 0, 2),
     // (Nx = 1024, one 128 KB tile buffer refilled during the last stage by
     // tensor copies: 0.226 ms per launch at 1024x512x256 against 0.222 for
     // the same scheme with cp.async, pass_b_pipe1 -- not registered)
@@ -80,6 +91,12 @@ const int kNumVariantsA_f64q = sizeof(kVariantsA_f64q) / sizeof(kVariantsA_f64q[
 const VariantB kVariantsB_f64q[] = {
     TB_ENTRY(double, 1, 512, 256, 0, 2),
     TB_ENTRY(double, 1, 512, 512, 0, 2),
+    // Nx = 384, 8-column tiles of 48 KB: 3-deep ring 0.192 ms per launch,
+    // 2-deep 0.210, the cp.async double buffer 0.216.  (Nx = 1024, one 128 KB
+    // buffer refilled during the last stage: 0.462 against 0.433 for the
+    // same scheme with cp.async -- not registered)
+    TB_ENTRY(double, 1, 384, 256, 0, 3),
+    TB_ENTRY(double, 1, 384, 256, 0, 2),
 };
 const int kNumVariantsB_f64q = sizeof(kVariantsB_f64q) / sizeof(kVariantsB_f64q[0]);
 

@@ -568,7 +568,7 @@ template <typename T, int NX, int NT, int NBUF>
 struct BShape {
     using V = cx_t<T>;
     static constexpr int W = 128 / (int)sizeof(V);
-    static constexpr int BOXH = NX > 256 ? 256 : NX;  // rows per tensor copy
+    static constexpr int BOXH = box_rows(NX);         // rows per tensor copy
     static constexpr int NBOX = (NX + BOXH - 1) / BOXH;
     static constexpr int TILE_BYTES = NX * W * (int)sizeof(V);
     static constexpr int BUF = (TILE_BYTES + 127) / 128 * 128;
@@ -576,6 +576,7 @@ struct BShape {
     static constexpr size_t smem_bytes() { return (size_t)TAB + (size_t)NBUF * BUF + NBUF * 8 + 128; }
     static constexpr int EPC = (int)sizeof(V) / 8;   // 8-byte elements per complex
     static_assert(NX % BOXH == 0, "whole boxes");
+    static_assert((BOXH * W * (int)sizeof(V)) % 128 == 0, "128-byte aligned box destinations");
 };
 
 template <typename T, int NX, int NT, bool FWD, int VARIANT, int NBUF, bool EPI>

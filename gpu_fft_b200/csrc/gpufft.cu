@@ -1019,7 +1019,7 @@ static int launch_pass_b(const Plan &P, void *data, cudaStream_t s, bool fwd, do
         CUtensorMap tm;
         const int epc = (int)sizeof(cx_t<T>) / 8;  // 8-byte elements per complex
         if (!encode_view(&tm, data, prm.ncols * epc, P.nx, prm.ncols * (long long)sizeof(cx_t<T>), P.fb->w * epc,
-                         (int)std::min<int64_t>(P.nx, 256)))
+                         q::box_rows((int)P.nx)))  // the kernel's rows per copy (BShape::BOXH)
             return set_error(GPUFFT_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Pass B field view");
         void *args[] = {&prm, &tm};
         const void *k = prm.epi ? (fwd ? P.fb->kfwd_epi : P.fb->kinv_epi) : (fwd ? P.fb->kfwd : P.fb->kinv);
