@@ -30,6 +30,7 @@ const VariantA kVariantsA_f32q[] = {
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),
+    QA_ENTRY(float, 0, 512, 128, 256, 0, 3, 16),
     // 360 x 240 planes (384 x 360 x 480): the row FFT is 16 x 15 (prime-factor
     // radix 15), 4-deep ring of 52 KB buffers; ms per launch: 20-row items on
     // 10 consumer warps 0.230 / 0.235 (an 11-warp CTA gets 168 registers a
