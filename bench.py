@@ -684,11 +684,12 @@ def run_precision(args, world, rank):
     out["fp32"] = {"ms": round(ms32, 4), "rel_l2_vs_fp64": e_l2, "max_err_rel_to_max": e_max,
                    "field_bytes": S32, "x_pass_ms": round(time_x_pass(p32, x32), 4), "plan": p32.describe()}
     del x32
-    # ---- FP32 storage, x-pass radix-16 stages on the tensor cores (split BF16)
+    # ---- FP32 storage, x-pass radix-16 stages on the tensor cores (tcgen05 with
+    # split TF32 operands, or mma.sync with split BF16 operands: the plan's pick)
     try:
         ptc = g.Plan(n, n, n, "float", autotune=not args.no_autotune, tc_split=True)
     except g.GpuFFTError as e:
-        out["tc_split_bf16"] = {"status": f"unsupported at {n}^3: {e}"}
+        out["tc_split"] = {"status": f"unsupported at {n}^3: {e}"}
         ptc = None
     if ptc is not None:
         xt = f64.float()
@@ -699,12 +700,14 @@ def run_precision(args, world, rank):
         del yt
         mst = time_fp32_plan(ptc, xt)
         xb = time_x_pass(ptc, xt)
-        out["tc_split_bf16"] = {"ms": round(mst, 4), "rel_l2_vs_fp64": t_l2, "max_err_rel_to_max": t_max,
-                                "rel_l2_vs_plain_fp32": vs_plain, "gate_vs_plain": 1e-6,
-                                "speedup_vs_fp32": round(ms32 / mst, 3), "field_bytes": S32,
-                                "x_pass_ms": round(xb, 4),
-                                "x_pass_speedup_vs_fp32": round(out["fp32"]["x_pass_ms"] / xb, 3),
-                                "plan": ptc.describe()}
+        desc = ptc.describe()
+        form = "tcgen05, split TF32 operands" if " v=3 " in desc else "mma.sync, split BF16 operands"
+        out["tc_split"] = {"form": form, "ms": round(mst, 4), "rel_l2_vs_fp64": t_l2, "max_err_rel_to_max": t_max,
+                           "rel_l2_vs_plain_fp32": vs_plain, "gate_vs_plain": 1e-6,
+                           "speedup_vs_fp32": round(ms32 / mst, 3), "field_bytes": S32,
+                           "x_pass_ms": round(xb, 4),
+                           "x_pass_speedup_vs_fp32": round(out["fp32"]["x_pass_ms"] / xb, 3),
+                           "plan": desc}
         del xt, ptc
     del y32
     # ---- 16-bit storage, per-pencil scales, FP32 butterflies
