@@ -54,9 +54,9 @@ NCU_TRAFFIC = {
     ((512, 512, 512, "float"), "pass_A_fwd",
      ("fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4 ", "split=0}")): 560_384_512 + 771_755_008,
     ((512, 512, 512, "float"), "pass_A_fwd",
-     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ")): 539_164_160 + 488_252_160,
+     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_180_288 + 639_723_008,
     ((512, 512, 512, "float"), "pass_A_inv",
-     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ")): 539_425_536 + 485_129_984,
+     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_134_464 + 542_402_816,
     ((512, 512, 512, "float"), "pass_B_fwd", ("fastB{kind=3 nx=512 w=16 nt=256 v=1 ", "smem=135312}")):
         539_003_904 + 480_740_608,
     ((512, 512, 512, "float"), "pass_B_inv", ("fastB{kind=3 nx=512 w=16 nt=256 v=1 ", "smem=135312}")):
@@ -624,7 +624,7 @@ def run_precision(args, world, rank):
     import torch
     import gpu_fft_b200 as g
 
-    n = args.nx if args.nx != NX else 1024
+    n = args.prec_n
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
     f64, p64 = turbulence_on_gpu(n)
@@ -1022,6 +1022,7 @@ def main():
                     default="headline",
                     help="headline: 512^3 R2C+C2R (the bench contract); batch64 / spectral: batched form; "
                          "precision: 16-bit storage form at 1024^3; serving: request loop under Poisson arrivals")
+    ap.add_argument("--prec-n", type=int, default=1024, help="cube side of the precision workload")
     ap.add_argument("--serve-requests", type=int, default=3000)
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.8, 1.0, 1.5, 2.5])
