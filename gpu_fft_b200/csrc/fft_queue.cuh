@@ -336,6 +336,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                             // once any CTA has given up, the others stop waiting too
                             if ((long long)(globaltimer() - t0) > P.wait_ns || ld_acquire(&ctr[2]) != 0) {
                                 err = true;  // go on: wrong results, no hang
+                                atomicExch(&ctr[2], 1);  // every other wait gives up at once
                                 break;
                             }
                         }

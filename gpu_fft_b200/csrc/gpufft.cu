@@ -366,6 +366,11 @@ static int setup_queue(Plan &P) {
     P.q_depth = depth;
     P.q_nitems = (int)fwd.size();
     P.q_need = nri;
+    // test hook of the bounded dependency wait: with GPUFFT_QUEUE_UNREACHABLE=1
+    // at plan creation every second-phase item waits for one first-phase item
+    // more than exist, so the wait runs out (GPUFFT_QUEUE_WAIT_MS, read at
+    // launch, sets the limit) and gpufft_plan_check reports it
+    if (const char *ev = std::getenv("GPUFFT_QUEUE_UNREACHABLE")) P.q_extra = std::atoi(ev) == 1 ? 1 : 0;
     P.q_items_f = reinterpret_cast<const int *>(b + cbytes);
     P.q_items_i = reinterpret_cast<const int *>(b + cbytes + lbytes);
     P.q_unp = b + cbytes + 2 * lbytes;
@@ -945,7 +950,7 @@ static int launch_pass_a(const Plan &P, void *data, cudaStream_t s, bool fwd, co
         qp.items = fwd ? P.q_items_f : P.q_items_i;
         qp.nitems = P.q_nitems;
         qp.ctr = reinterpret_cast<int *>(P.q_dev);
-        qp.need = fwd ? P.q_need : (int)((P.nz / 2) / wy);
+        qp.need = (fwd ? P.q_need : (int)((P.nz / 2) / wy)) + P.q_extra;
         qp.wait_ns = 2000000000LL;  // 2 s: far above any launch's length
         if (const char *ev = std::getenv("GPUFFT_QUEUE_WAIT_MS")) qp.wait_ns = 1000000LL * std::max(1, std::atoi(ev));
         void *args[] = {&qp, &tm[0], &tm[1], &tm[2]};

@@ -38,6 +38,7 @@ struct Plan {
     int q_depth = 0;     // planes between a plane's first and second phase in the lists
     int q_nitems = 0;    // items per launch
     int q_need = 0;      // first-phase items per plane (forward)
+    int q_extra = 0;     // test hook: items a plane's second phase waits for beyond those that exist
     const int *q_items_f = nullptr, *q_items_i = nullptr;
     const void *q_unp = nullptr;    // forward unpack factors
     const void *q_unp_i = nullptr;  // inverse pack factors
