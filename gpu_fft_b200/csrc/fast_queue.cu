@@ -42,12 +42,15 @@ const VariantA kVariantsA_f32q[] = {
 };
 const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[0]);
 
-// Pass B fed by tensor copies: (Nx, consumer threads, radix variant, ring depth)
-#define TB_ENTRY(T, DT, NX, NT, V, NBUF)                                                                          \
-    {3, DT, NX, q::BShape<T, NX, NT, NBUF>::W, NT, V, q::BShape<T, NX, NT, NBUF>::smem_bytes(),                  \
-     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, false>,                                                \
-     (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, false>,                                               \
-     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, true>, (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, true>}
+// Pass B fed by tensor copies: (Nx, consumer threads, radix variant, ring depth
+// [, columns per tile: 128-byte rows when omitted])
+#define TB_ENTRY_W(T, DT, NX, NT, V, NBUF, WW)                                                                    \
+    {3, DT, NX, q::BShape<T, NX, NT, NBUF, WW>::W, NT, V, q::BShape<T, NX, NT, NBUF, WW>::smem_bytes(),          \
+     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, false, WW>,                                            \
+     (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, false, WW>,                                           \
+     (const void *)q::pass_b_tma<T, NX, NT, true, V, NBUF, true, WW>,                                             \
+     (const void *)q::pass_b_tma<T, NX, NT, false, V, NBUF, true, WW>}
+#define TB_ENTRY(T, DT, NX, NT, V, NBUF) TB_ENTRY_W(T, DT, NX, NT, V, NBUF, 0)
 
 const VariantB kVariantsB_f32q[] = {
     // 512^3 on B200, ms per launch (fwd / inv): 2-deep ring 0.184 / 0.183,
@@ -69,6 +72,11 @@ const VariantB kVariantsB_f32q[] = {
     TB_ENTRY(float, 0, 384, 256, 0, 3),
     TB_ENTRY(float, 0, 384, 256, 0, 2),
     TB_ENTRY(float, 0, 384, 512, 0, 2),
+    // (Nx = 1024, 8-column tiles of 64-byte rows in a 2-deep ring of 64 KB,
+    // TB_ENTRY_W(float, 0, 1024, 256, 0, 2, 8): 0.216 ms per launch at
+    // 1024x512x256 against 0.221 for pass_b_pipe1, but 3.36 against 1.85 ms
+    // at 1024^3, where the two halves of a 128-byte line no longer meet in
+    // L2 -- not registered)
     // (Nx = 1024, one 128 KB tile buffer refilled during the last stage by
     // tensor copies: 0.226 ms per launch at 1024x512x256 against 0.222 for
     // the same scheme with cp.async, pass_b_pipe1 -- not registered)
@@ -98,6 +106,8 @@ const VariantB kVariantsB_f64q[] = {
     // same scheme with cp.async -- not registered)
     TB_ENTRY(double, 1, 384, 256, 0, 3),
     TB_ENTRY(double, 1, 384, 256, 0, 2),
+    // (Nx = 1024, 4-column tiles of 64-byte rows in a 2-deep ring: 0.535 ms
+    // per launch at 1024x512x256 against 0.432 for pass_b_pipe1 -- not registered)
 };
 const int kNumVariantsB_f64q = sizeof(kVariantsB_f64q) / sizeof(kVariantsB_f64q[0]);
 

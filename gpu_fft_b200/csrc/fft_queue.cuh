@@ -565,10 +565,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
 // (2 s), the CTA stops, waits for its copies still in flight (bounded),
 // frees the tensor memory and raises P.err.
 // ---------------------------------------------------------------------------
-template <typename T, int NX, int NT, int NBUF>
+template <typename T, int NX, int NT, int NBUF, int WW = 0>
 struct BShape {
     using V = cx_t<T>;
-    static constexpr int W = 128 / (int)sizeof(V);
+    static constexpr int W = WW > 0 ? WW : 128 / (int)sizeof(V);  // columns per tile (128-byte rows by default)
     static constexpr int BOXH = box_rows(NX);         // rows per tensor copy
     static constexpr int NBOX = (NX + BOXH - 1) / BOXH;
     static constexpr int TILE_BYTES = NX * W * (int)sizeof(V);
@@ -580,9 +580,9 @@ struct BShape {
     static_assert((BOXH * W * (int)sizeof(V)) % 128 == 0, "128-byte aligned box destinations");
 };
 
-template <typename T, int NX, int NT, bool FWD, int VARIANT, int NBUF, bool EPI>
+template <typename T, int NX, int NT, bool FWD, int VARIANT, int NBUF, bool EPI, int WW = 0>
 __global__ void __launch_bounds__(NT, 1) pass_b_tma(const PassBParams P, const __grid_constant__ CUtensorMap tm) {
-    using S = BShape<T, NX, NT, NBUF>;
+    using S = BShape<T, NX, NT, NBUF, WW>;
     using V = cx_t<T>;
     using FFT = TileFFT<T, NX, S::W, NT, FWD, COLS, VARIANT, fast::BLOCK>;
     static_assert(!FFT::kTcStage, "the tensor-core stage uses its own swizzled layout");
