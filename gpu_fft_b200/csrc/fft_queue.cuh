@@ -132,6 +132,15 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+// 1D bulk copy shared -> global (same alignment rules), committed as one bulk group
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// this thread's bulk stores have read their shared-memory sources / have completed
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 // 2D tensor copy global -> shared of the box at (x, y) of `map` (no multicast)
 __device__ __forceinline__ void tensor_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
     asm volatile(
@@ -289,10 +298,23 @@ __global__ void __launch_bounds__(NT + 32, 1)
             // Items are published in claim order; `pub` is the next one.  The
             // dependency wait below keeps publishing the CTA's own finished
             // items, so it never waits on an item of its own CTA.
+            // The inverse's row items (the second phase: nothing waits for
+            // them) leave their real rows in the buffer; this warp writes the
+            // span back with one bulk store, and waits for it to have read the
+            // buffer before the buffer is refilled (stores_out).
             int pub = 0;
+            bool stores_out = false;
             auto publish = [&](int j) {
                 const int code = info[j % NBUF];
-                if (code >= 0 && ((code >> 15) & 1) == first_type) red_release_add(&ctr[4 + (code >> 16)], 1);
+                if (code < 0) return;
+                const int type = (code >> 15) & 1;
+                if (type == first_type) {
+                    red_release_add(&ctr[4 + (code >> 16)], 1);
+                } else if (!FWD && type == ROW_ITEM) {
+                    const long long row0 = (long long)(code >> 16) * NY + (long long)(code & 0x7fff) * RI;
+                    bulk_store(field + row0 * NH, bufs + (size_t)(j % NBUF) * S::BUF, (uint32_t)S::ROW_BYTES);
+                    stores_out = true;
+                }
             };
             // publish items < upto that are finished, without waiting
             auto try_publish = [&](int upto) {
@@ -344,6 +366,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     fence_proxy_async_global();
                 }
                 fence_proxy_async_shared();  // the consumers' accesses to buffer s come first
+                if (stores_out) {
+                    bulk_wait_read();  // a bulk store from buffer s has read it
+                    stores_out = false;
+                }
                 unsigned char *b = bufs + (size_t)s * S::BUF;
                 if (type == ROW_ITEM) {
                     mbar_arrive_expect_tx(&full[s], (uint32_t)S::ROW_BYTES);
@@ -371,6 +397,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     }
                 }
             }
+            bulk_wait_all();  // every row this CTA stored is in global memory before it exits
             if (err) atomicExch(&ctr[2], 1);
         }
     } else {
@@ -450,13 +477,15 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         x[j] = c_add(c_add(xa, cm), c_mul(c_sub(xa, cm), unp[kk]));
                     }
                     row_step1<false, R2>(x, row, rtw, a);
+                    V y[16];
+                    if (R2 == 16 || a < R2) row_step2<false>(y, row, a);
+                    __syncwarp();  // step 2's reads are done before the real row is stored in place
                     if (R2 == 16 || a < R2) {
-                        V y[16];
-                        row_step2<false>(y, row, a);
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) st_g(grow + a + R2 * j, y[j]);
+                        for (int j = 0; j < 16; ++j) row[a + R2 * j] = y[j];
                     }
-                    if (a == 0) st_g(grow + M, V{(T)0, (T)0});  // padding cells of the real row
+                    if (a == 0) row[M] = V{(T)0, (T)0};  // padding cells of the real row
+                    fence_proxy_async_shared();  // the copy warp's bulk store reads the row
                 }
             } else {
                 // column item: y FFT of columns c0 .. c0 + WY - 1 of all NY rows
