@@ -8,10 +8,13 @@ namespace gpufft {
 namespace fast {
 
 // (Ny, Nz/2, consumer threads, y radix variant, ring depth, columns per column item)
-#define QA_ENTRY(T, DT, NY, M, NT, VY, NBUF, WY)                                                                \
+// (QA_ENTRY_FB: the forward's row items written back by bulk stores as well)
+#define QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, FB)                                                          \
     {2, NBUF, DT, NY, M, 2, WY, NT + 32, VY, 0, q::QShape<T, NY, M, NT, NBUF, WY>::smem_bytes(),                \
-     (const void *)q::pass_a_queue<T, NY, M, NT, true, VY, NBUF, WY>,                                           \
-     (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY>, nullptr, nullptr}
+     (const void *)q::pass_a_queue<T, NY, M, NT, true, VY, NBUF, WY, FB>,                                       \
+     (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY, FB>, nullptr, nullptr}
+#define QA_ENTRY(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, false)
+#define QA_ENTRY_FB(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, true)
 
 const VariantA kVariantsA_f32q[] = {
     // 512^2 planes, B200, ms per launch at 512^3 (forward / inverse, queue
@@ -24,8 +27,13 @@ const VariantA kVariantsA_f32q[] = {
     // two groups of 8 consumer warps, each on its own 16-row or 8-column
     // items (barrier waits of one group overlapping the other's work), 4- or
     // 5-deep ring of 40 KB buffers 0.467-0.476 / 0.484-0.492
-    QA_ENTRY(float, 0, 512, 256, 512, 0, 3, 16),
-    QA_ENTRY(float, 0, 512, 256, 512, 0, 2, 16),
+    // Row items of both directions written back by bulk stores from the copy
+    // warp: 0.369 / 0.369 (forward by the consumers' own stores 0.384, and
+    // 0.408 for the inverse before its rows went by bulk store too).  At
+    // 512 x 128 and in FP64 the forward's bulk stores were slower (the copy
+    // warp waits for each before it publishes): 0.470 against 0.443 ms.
+    QA_ENTRY_FB(float, 0, 512, 256, 512, 0, 3, 16),
+    QA_ENTRY_FB(float, 0, 512, 256, 512, 0, 2, 16),
 
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442

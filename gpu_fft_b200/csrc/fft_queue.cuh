@@ -249,7 +249,10 @@ __device__ __forceinline__ void row_step2(V (&y)[16], const V *row, int b) {
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
-template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16>
+// FB: the forward's row items are also written back by bulk stores (the
+// inverse's always are); the copy warp then waits for each store before it
+// publishes the item.
+template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16, bool FB = false>
 __global__ void __launch_bounds__(NT + 32, 1)
     pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
                  const __grid_constant__ CUtensorMap tm_x) {
@@ -298,23 +301,27 @@ __global__ void __launch_bounds__(NT + 32, 1)
             // Items are published in claim order; `pub` is the next one.  The
             // dependency wait below keeps publishing the CTA's own finished
             // items, so it never waits on an item of its own CTA.
-            // The inverse's row items (the second phase: nothing waits for
-            // them) leave their real rows in the buffer; this warp writes the
+            // Row items leave their rows in the buffer; this warp writes the
             // span back with one bulk store, and waits for it to have read the
-            // buffer before the buffer is refilled (stores_out).
+            // buffer before the buffer is refilled (stores_out).  A forward
+            // row item is a first-phase item: its store completes, and is
+            // ordered before the release, before the item is published.
             int pub = 0;
             bool stores_out = false;
             auto publish = [&](int j) {
                 const int code = info[j % NBUF];
                 if (code < 0) return;
                 const int type = (code >> 15) & 1;
-                if (type == first_type) {
-                    red_release_add(&ctr[4 + (code >> 16)], 1);
-                } else if (!FWD && type == ROW_ITEM) {
+                if (type == ROW_ITEM && (!FWD || FB)) {
                     const long long row0 = (long long)(code >> 16) * NY + (long long)(code & 0x7fff) * RI;
                     bulk_store(field + row0 * NH, bufs + (size_t)(j % NBUF) * S::BUF, (uint32_t)S::ROW_BYTES);
                     stores_out = true;
+                    if (FWD) {
+                        bulk_wait_all();
+                        fence_proxy_async_global();
+                    }
                 }
+                if (type == first_type) red_release_add(&ctr[4 + (code >> 16)], 1);
             };
             // publish items < upto that are finished, without waiting
             auto try_publish = [&](int upto) {
@@ -446,6 +453,9 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     // unpack: X[k] = E + O, E = (Z[k] + conj Z[M-k]) / 2,
                     // O = -i w^k (Z[k] - conj Z[M-k]) / 2 = (Z[k] - conj Z[M-k]) u_k with
                     // the table u_k = -i w^k / 2; bins 0 and M packed in slot 0
+                    // (with FB every bin goes into x[] first: the row is
+                    // overwritten in place after the warp's partner reads, and the
+                    // copy warp writes the span back with one bulk store)
                     const T hf = (T)0.5;
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
@@ -455,11 +465,17 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         const V e2 = c_add(za, zb);
                         const V o = c_mul(c_sub(za, zb), unp[kk]);
                         const V xa = V{fma(hf, e2.x, o.x), fma(hf, e2.y, o.y)};
-                        if (kk == 0) {
-                            st_g(grow, V{xa.x, fma(hf, e2.x, -o.x)});  // (Re X0, Re XM)
-                        } else {
-                            st_g(grow + kk, xa);
-                        }
+                        const V xs = kk == 0 ? V{xa.x, fma(hf, e2.x, -o.x)} : xa;  // slot 0: (Re X0, Re XM)
+                        if constexpr (FB)
+                            x[j] = xs;
+                        else
+                            st_g(grow + kk, xs);
+                    }
+                    if constexpr (FB) {
+                        __syncwarp();
+#pragma unroll
+                        for (int j = 0; j < R2; ++j) row[a + 16 * j] = x[j];
+                        fence_proxy_async_shared();  // the copy warp's bulk store reads the row
                     }
                 } else {
                     // pack: Z[k] = S + Pk, S = X[k] + conj X[M-k], Pk = i conj(w^k) (X[k] - conj X[M-k]);
