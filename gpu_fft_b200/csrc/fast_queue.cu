@@ -13,8 +13,8 @@ namespace fast {
     {2, NBUF, DT, NY, M, 2, WY, NT + 32, VY, 0, q::QShape<T, NY, M, NT, NBUF, WY>::smem_bytes(),                \
      (const void *)q::pass_a_queue<T, NY, M, NT, true, VY, NBUF, WY, FB>,                                       \
      (const void *)q::pass_a_queue<T, NY, M, NT, false, VY, NBUF, WY, FB>, nullptr, nullptr}
-#define QA_ENTRY(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, false)
-#define QA_ENTRY_FB(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, true)
+#define QA_ENTRY(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, 0)
+#define QA_ENTRY_FB(T, DT, NY, M, NT, VY, NBUF, WY) QA_ENTRY_X(T, DT, NY, M, NT, VY, NBUF, WY, 1)
 
 const VariantA kVariantsA_f32q[] = {
     // 512^2 planes, B200, ms per launch at 512^3 (forward / inverse, queue
@@ -32,11 +32,15 @@ const VariantA kVariantsA_f32q[] = {
     // 0.408 for the inverse before its rows went by bulk store too).  At
     // 512 x 128 and in FP64 the forward's bulk stores were slower (the copy
     // warp waits for each before it publishes): 0.470 against 0.443 ms.
-    QA_ENTRY_FB(float, 0, 512, 256, 512, 0, 3, 16),
-    QA_ENTRY_FB(float, 0, 512, 256, 512, 0, 2, 16),
+    // The inverse's column items with their even rows by tensor store as
+    // well: inverse 0.354 (forward with the same: 0.371 against 0.369).
+    QA_ENTRY_X(float, 0, 512, 256, 512, 0, 3, 16, 3),
+    QA_ENTRY_X(float, 0, 512, 256, 512, 0, 2, 16, 3),
 
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
+    // (the inverse's column items with their even rows by tensor store:
+    // 0.433 against 0.431 -- not registered)
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),
     QA_ENTRY(float, 0, 512, 128, 256, 0, 3, 16),
     // 360 x 240 planes (384 x 360 x 480): the row FFT is 16 x 15 (prime-factor

@@ -141,6 +141,14 @@ __device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t 
 // this thread's bulk stores have read their shared-memory sources / have completed
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// 2D tensor copy shared -> global of the box at (x, y) of `map`, committed as one bulk group
+__device__ __forceinline__ void tensor_store_2d(const CUtensorMap *map, int x, int y, const void *src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
 // 2D tensor copy global -> shared of the box at (x, y) of `map` (no multicast)
 __device__ __forceinline__ void tensor_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
     asm volatile(
@@ -249,10 +257,14 @@ __device__ __forceinline__ void row_step2(V (&y)[16], const V *row, int b) {
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
-// FB: the forward's row items are also written back by bulk stores (the
-// inverse's always are); the copy warp then waits for each store before it
-// publishes the item.
-template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16, bool FB = false>
+// FB bit 0: the forward's row items are also written back by bulk stores
+// (the inverse's always are); the copy warp then waits for each store before
+// it publishes the item.  FB bit 1 (inverse, row-pair view only): a column
+// item's even rows go back by one tensor store of box E from the copy warp
+// (the odd rows, which start 8 bytes off a 16-byte boundary, by the
+// consumers' own stores); in the forward the barrier it needs cost more than
+// the stores it saves.
+template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16, int FB = 0>
 __global__ void __launch_bounds__(NT + 32, 1)
     pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
                  const __grid_constant__ CUtensorMap tm_x) {
@@ -288,6 +300,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
     int *ctr = P.ctr;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int first_type = FWD ? ROW_ITEM : COL_ITEM;  // the phase that publishes
+    constexpr bool CT = (FB & 2) != 0 && S::PAIR && !FWD;
 
     if (warp == NT / 32) {
         // ------------------------------ producer ------------------------------
@@ -312,11 +325,18 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 const int code = info[j % NBUF];
                 if (code < 0) return;
                 const int type = (code >> 15) & 1;
-                if (type == ROW_ITEM && (!FWD || FB)) {
+                if (type == ROW_ITEM && (!FWD || (FB & 1))) {
                     const long long row0 = (long long)(code >> 16) * NY + (long long)(code & 0x7fff) * RI;
                     bulk_store(field + row0 * NH, bufs + (size_t)(j % NBUF) * S::BUF, (uint32_t)S::ROW_BYTES);
                     stores_out = true;
                     if (FWD) {
+                        bulk_wait_all();
+                        fence_proxy_async_global();
+                    }
+                } else if (type == COL_ITEM && CT && !(FWD && (code & 0x7fff) == 0)) {
+                    tensor_store_2d(&tm_e, (code & 0x7fff) * WY, (code >> 16) * BH, bufs + (size_t)(j % NBUF) * S::BUF);
+                    stores_out = true;
+                    if (!FWD) {
                         bulk_wait_all();
                         fence_proxy_async_global();
                     }
@@ -466,12 +486,12 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         const V o = c_mul(c_sub(za, zb), unp[kk]);
                         const V xa = V{fma(hf, e2.x, o.x), fma(hf, e2.y, o.y)};
                         const V xs = kk == 0 ? V{xa.x, fma(hf, e2.x, -o.x)} : xa;  // slot 0: (Re X0, Re XM)
-                        if constexpr (FB)
+                        if constexpr ((FB & 1) != 0)
                             x[j] = xs;
                         else
                             st_g(grow + kk, xs);
                     }
-                    if constexpr (FB) {
+                    if constexpr ((FB & 1) != 0) {
                         __syncwarp();
 #pragma unroll
                         for (int j = 0; j < R2; ++j) row[a + 16 * j] = x[j];
@@ -522,6 +542,16 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     }
                 };
                 auto dst = [&](int n, int w, V v) { st_g(gplane + (long long)n * NH + c0 + w, v); };
+                // CT: even rows into box E's place at the start of the buffer, once
+                // a barrier (the hook's) has ended the last stage's reads of the tile
+                V *ew = reinterpret_cast<V *>(b);
+                auto dst_ct = [&](int n, int w, V v) {
+                    if (n & 1)
+                        st_g(gplane + (long long)n * NH + c0 + w, v);
+                    else
+                        ew[(n >> 1) * WY + w] = v;
+                };
+                auto after_reads = [] {};
                 // the y FFT in place in the buffer; returns where a ToSmem result lies
                 auto colfft = [&](auto &src_, auto &dst_) -> V * {
                     ColFFT::run(src_, dst_, tile, sty);
@@ -530,7 +560,12 @@ __global__ void __launch_bounds__(NT + 32, 1)
                 if constexpr (FWD) {
                     auto src = [&](int n, int w) -> V { return at(n, w); };
                     if (sub != 0) {
-                        colfft(src, dst);
+                        if constexpr (CT) {
+                            ColFFT::run(src, dst_ct, tile, sty, after_reads);
+                            fence_proxy_async_shared();  // the copy warp's tensor store reads box E
+                        } else {
+                            colfft(src, dst);
+                        }
                     } else {
                         // column 0 carries (bin 0) + i (bin M); split after the FFT
                         ToSmem ts;
@@ -569,7 +604,12 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         }
                         return at(n, w);
                     };
-                    colfft(src, dst);
+                    if constexpr (CT) {
+                        ColFFT::run(src, dst_ct, tile, sty, after_reads);
+                        fence_proxy_async_shared();  // the copy warp's tensor store reads box E
+                    } else {
+                        colfft(src, dst);
+                    }
                 }
             }
             group_sync<NT>();  // stores issued, buffer reads done
