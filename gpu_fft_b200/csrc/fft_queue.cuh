@@ -259,11 +259,11 @@ __device__ __forceinline__ void row_step2(V (&y)[16], const V *row, int b) {
 // ---------------------------------------------------------------------------
 // FB bit 0: the forward's row items are also written back by bulk stores
 // (the inverse's always are); the copy warp then waits for each store before
-// it publishes the item.  FB bit 1 (inverse, row-pair view only): a column
-// item's even rows go back by one tensor store of box E from the copy warp
-// (the odd rows, which start 8 bytes off a 16-byte boundary, by the
-// consumers' own stores); in the forward the barrier it needs cost more than
-// the stores it saves.
+// it publishes the item.  FB bits 1 (inverse) and 2 (forward): a column
+// item's results go back by tensor stores of its E boxes from the copy warp
+// -- with the row-pair view (FP32) only the even rows (the odd ones start 8
+// bytes off a 16-byte boundary and are stored by the consumers), with the
+// single-row view (FP64) every row; it needs one more barrier per item.
 template <typename T, int NY, int M, int NT, bool FWD, int VY, int NBUF, int WY_ = 16, int FB = 0>
 __global__ void __launch_bounds__(NT + 32, 1)
     pass_a_queue(const PassAQParams P, const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_o,
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
     int *ctr = P.ctr;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int first_type = FWD ? ROW_ITEM : COL_ITEM;  // the phase that publishes
-    constexpr bool CT = (FB & 2) != 0 && S::PAIR && !FWD;
+    constexpr bool CT = (FB & (FWD ? 4 : 2)) != 0;
 
     if (warp == NT / 32) {
         // ------------------------------ producer ------------------------------
@@ -334,7 +334,16 @@ __global__ void __launch_bounds__(NT + 32, 1)
                         fence_proxy_async_global();
                     }
                 } else if (type == COL_ITEM && CT && !(FWD && (code & 0x7fff) == 0)) {
-                    tensor_store_2d(&tm_e, (code & 0x7fff) * WY, (code >> 16) * BH, bufs + (size_t)(j % NBUF) * S::BUF);
+                    unsigned char *src = bufs + (size_t)(j % NBUF) * S::BUF;
+                    if constexpr (S::PAIR) {
+                        tensor_store_2d(&tm_e, (code & 0x7fff) * WY, (code >> 16) * BH, src);
+                    } else {
+                        constexpr int EPC = (int)sizeof(V) / 8;
+#pragma unroll
+                        for (int q = 0; q < S::NBX; ++q)
+                            tensor_store_2d(&tm_e, EPC * (code & 0x7fff) * WY, (code >> 16) * NY + q * S::BHT,
+                                            src + (size_t)q * S::BHT * WY * sizeof(V));
+                    }
                     stores_out = true;
                     if (!FWD) {
                         bulk_wait_all();
@@ -542,14 +551,18 @@ __global__ void __launch_bounds__(NT + 32, 1)
                     }
                 };
                 auto dst = [&](int n, int w, V v) { st_g(gplane + (long long)n * NH + c0 + w, v); };
-                // CT: even rows into box E's place at the start of the buffer, once
-                // a barrier (the hook's) has ended the last stage's reads of the tile
+                // CT: rows into the E boxes' place at the start of the buffer, once a
+                // barrier (the hook's) has ended the last stage's reads of the tile
                 V *ew = reinterpret_cast<V *>(b);
                 auto dst_ct = [&](int n, int w, V v) {
-                    if (n & 1)
-                        st_g(gplane + (long long)n * NH + c0 + w, v);
-                    else
-                        ew[(n >> 1) * WY + w] = v;
+                    if constexpr (S::PAIR) {
+                        if (n & 1)
+                            st_g(gplane + (long long)n * NH + c0 + w, v);
+                        else
+                            ew[(n >> 1) * WY + w] = v;
+                    } else {
+                        ew[n * WY + w] = v;
+                    }
                 };
                 auto after_reads = [] {};
                 // the y FFT in place in the buffer; returns where a ToSmem result lies
