@@ -65,7 +65,9 @@ const int kNumVariantsA_f32q = sizeof(kVariantsA_f32q) / sizeof(kVariantsA_f32q[
 #define TB_ENTRY(T, DT, NX, NT, V, NBUF) TB_ENTRY_W(T, DT, NX, NT, V, NBUF, 0)
 
 const VariantB kVariantsB_f32q[] = {
-    // 512^3 on B200, ms per launch (fwd / inv): 2-deep ring 0.184 / 0.183,
+    // 512^3 on B200, ms per launch (fwd / inv): 2-deep ring 0.184 / 0.183
+    // (the tile written back in place and stored by tensor copies from thread
+    // 0, its buffer refilled one tile later in a 3-deep ring: 0.192-0.195),
     // 3-deep 0.211 / 0.210 (256 threads) and 0.207 / 0.207 (512 threads),
     // against 0.204 / 0.203 for the cp.async double buffer
     TB_ENTRY(float, 0, 512, 256, 1, 2),
