@@ -83,6 +83,9 @@ const VariantB kVariantsB_f32q[] = {
     // GPUFFT_PLAN_TC_SPLIT use it.  512^3: 0.360 / 0.360 ms, 1.8e-7 from the
     // plain pass (mma.sync forms 0.427-0.503 ms).  Fusing Xh [Bh | Bl] into
     // N = 64 MMAs with per-block barriers: 0.374 ms and 3.8e-7, not kept.
+    // Pipelining tiles in a 3-deep ring (tile k's first tensor-core stage on
+    // the tensor cores while the CTA runs tile k-1's last stage): 0.365 ms,
+    // no better, not kept.
     TB_ENTRY(float, 0, 512, 512, 3, 2),
     // Nx = 384 (384 x 360 x 480): two boxes of 192 rows per tile; ms per
     // launch: 3-deep ring 0.0945, 2-deep 0.103 (256 or 512 threads), against
