@@ -40,6 +40,14 @@
 // mbarrier pairs), so an item's loads are in flight while the consumers
 // transform the previous one and no load occupies a register.
 //
+// Write-back.  Consumers store column items (and, unless FB says otherwise,
+// the forward's row items) with their own stores.  The inverse's row items,
+// and per FB the forward's row items and the column items' E boxes, are
+// left in the buffer and written back by the producer with one bulk or
+// tensor store per item; it waits for a store to have read the buffer before
+// refilling it, for a first-phase item's store to complete before publishing
+// the item, and for all its stores before the CTA exits.
+//
 // Deadlock freedom: a CTA waits for a plane only in its producer, while its
 // consumers finish every item the CTA claimed earlier (they never wait on
 // anything but copies already issued) and the producer keeps publishing them
