@@ -40,7 +40,9 @@ const VariantA kVariantsA_f32q[] = {
     // 512 x 128 planes (1024 x 512 x 256): the row FFT is 16 x 8; queue depth
     // 32: 0.464 / 0.445 ms (depth 16: 0.517 / 0.626), the cluster form 0.484 / 0.442
     // (the inverse's column items with their even rows by tensor store:
-    // 0.433 against 0.431 -- not registered)
+    // 0.433 against 0.431; four rows per warp, 8 lanes a row, so that no lane
+    // idles in the radix-16 step: 0.456 / 0.440 against 0.449 / 0.430 --
+    // not registered)
     QA_ENTRY(float, 0, 512, 128, 512, 0, 3, 16),
     QA_ENTRY(float, 0, 512, 128, 256, 0, 3, 16),
     // 360 x 240 planes (384 x 360 x 480): the row FFT is 16 x 15 (prime-factor
