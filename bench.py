@@ -54,9 +54,9 @@ NCU_TRAFFIC = {
     ((512, 512, 512, "float"), "pass_A_fwd",
      ("fastA{kind=0 ny=512 m=256 rw=2 wy=16 nt=256 K=4 ", "split=0}")): 560_384_512 + 771_755_008,
     ((512, 512, 512, "float"), "pass_A_fwd",
-     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_256_576 + 597_823_232,
+     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_265_536 + 571_380_992,
     ((512, 512, 512, "float"), "pass_A_inv",
-     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_448_064 + 569_750_784,
+     ("fastA{kind=2 ny=512 m=256 rw=2 wy=16 nt=544 ", "smem=229564 ", "depth=32 ")): 539_431_168 + 568_524_288,
     ((512, 512, 512, "float"), "pass_B_fwd", ("fastB{kind=3 nx=512 w=16 nt=256 v=1 ", "smem=135312}")):
         539_003_904 + 480_740_608,
     ((512, 512, 512, "float"), "pass_B_inv", ("fastB{kind=3 nx=512 w=16 nt=256 v=1 ", "smem=135312}")):
