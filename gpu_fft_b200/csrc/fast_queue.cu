@@ -112,16 +112,22 @@ const int kNumVariantsB_f32q = sizeof(kVariantsB_f32q) / sizeof(kVariantsB_f32q[
 const VariantA kVariantsA_f64q[] = {
     // the forward's column items written back by tensor stores of every row
     // from the copy warp: forward 0.769 against 0.801 ms (the inverse's the
-    // same way: 0.797 against 0.786 -- not used)
+    // same way: 0.797 against 0.786 -- not used); the forward's row items by
+    // bulk stores as well, each awaited at the end of the copy warp's
+    // iteration: forward 0.720
+    QA_ENTRY_X(double, 1, 512, 256, 256, 0, 2, 8, 5),
     QA_ENTRY_X(double, 1, 512, 256, 256, 0, 2, 8, 4),
     QA_ENTRY(double, 1, 512, 256, 256, 0, 2, 8),
     // 512 x 128 planes (1024 x 512 x 256): two 74 KB buffers
-    // (forward column items by tensor stores: 0.966 against 1.001 ms forward)
+    // (forward column items by tensor stores: 0.966 against 1.001 ms forward;
+    // and the forward's row items by bulk stores: 0.921)
+    QA_ENTRY_X(double, 1, 512, 128, 256, 0, 2, 8, 5),
     QA_ENTRY_X(double, 1, 512, 128, 256, 0, 2, 8, 4),
     QA_ENTRY(double, 1, 512, 128, 256, 0, 2, 8),
     // 360 x 240 planes (384 x 360 x 480): 12-row items on 6 consumer warps,
     // two boxes of 180 rows per column item, 2- or 3-deep ring of 51 KB buffers
-    // (forward column items by tensor stores: 0.440 against 0.454 ms forward)
+    // (forward column items by tensor stores: 0.440 against 0.454 ms forward;
+    // the forward's row items by bulk stores as well: 0.447 -- not used)
     QA_ENTRY_X(double, 1, 360, 240, 192, 0, 3, 8, 4),
     QA_ENTRY(double, 1, 360, 240, 192, 0, 3, 8),
     QA_ENTRY(double, 1, 360, 240, 192, 0, 2, 8),
